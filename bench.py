@@ -1,0 +1,413 @@
+#!/usr/bin/env python
+"""SpMM benchmark on B200: plain FP32 SpMM of the 262,144-row power-law graph
+(~1.23M nonzeros, preferential-attachment columns) with a dense 262,144 x 128
+B, row-major, through libdaspmm's C ABI.  One step = one SpMM call.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  Multi-GPU: one process per GPU (torchrun);
+each rank owns a 262,144-row shard of a vertically stacked matrix (seeded by
+rank) with B replicated -- no data-path collective; weak scaling.
+
+--impl reference times the reference's own CPU implementation of the path
+(cpuSpmvReference, spmvspmm_benchmark.cu:11-39, built from the unmodified
+reference into oracle/_ref/libref.so; the oracle's restatement where that
+library is absent) on all host cores, on a bounded row sample per step.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "da-spmmul-kernel_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+NR = 262144
+NV = 128
+METRIC = "SpMM GFLOP/s"
+UNIT = "GFLOP/s"
+L2_BYTES = 126 * 1024 * 1024
+FALLBACK_HBM_GBS = 6650.0
+
+
+def workload_name(alg_name: str) -> str:
+    return (f"power-law graph 262144x262144 (~1.23M nnz, out-degree (k+0.16)^-2.1 on [1,4096], "
+            f"preferential attachment), B 262144x128 FP32 row-major, alg {alg_name}")
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs, burst copy)"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback (6.65 TB/s, earlier pool measurement)"
+
+
+def committed_traffic():
+    """dram bytes per launch of the main kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "k_bal_powerlaw262k_n128_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of SM clock and throttle reasons."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str | None):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines = []
+        self.t_on = None
+
+    def start(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+               "-lms", "200"]
+        if self.gpu_id:
+            cmd += ["-i", self.gpu_id]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.t_on = threading.Thread(target=self._read, daemon=True)
+        self.t_on.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append((time.time(), line.strip()))
+
+    def stop(self):
+        if self.proc is None:
+            return
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.t_on:
+            self.t_on.join(timeout=2)
+
+    def summary(self, t0=None, t1=None):
+        rows = []
+        for t, ln in self.lines:
+            if t0 is not None and (t < t0 or t > t1):
+                continue
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                rows.append((float(parts[0]), float(parts[1]), parts[4:8]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r)
+                          if v.lower().startswith("active")})
+        return {"sm_mhz": statistics.median(r[0] for r in rows),
+                "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ---------------------------------------------------------------- helpers
+def algorithmic_bytes(A, nv: int, s_val=4, s_b=4, s_c=4) -> int:
+    """nnz*(idx+val) + rowPtr + distinct B rows * nv * s_B + C writes."""
+    return (A.nnz * (4 + s_val) + 4 * (A.nr + 1) + A.cols_touched() * nv * s_b
+            + A.nr * nv * s_c)
+
+
+def cpu_reference_time(A, B, nv, nthreads, reps, row_sample=None):
+    """ms per pass of the reference's cpuSpmvReference (or the oracle port)."""
+    import numpy as np
+    from oracle import oracle as O
+    if row_sample is not None and row_sample < A.nr:
+        rp = A.rowPtr[: row_sample + 1].copy()
+        nnz = int(rp[-1])
+        ci, va = A.colIdx[:nnz], A.values[:nnz]
+        nr = row_sample
+    else:
+        rp, ci, va, nr, nnz = A.rowPtr, A.colIdx, A.values, A.nr, A.nnz
+    if O.ref_available():
+        R = O.ref()
+        ms = R.ref_cpu_bench(0, nr, A.nc, nnz, nv, O._p(rp), O._p(ci), O._p(va), O._p(B),
+                             nthreads, reps)
+        return ms, nnz, nr, "reference", nthreads
+    # oracle restatement, single thread
+    times = []
+    for _ in range(max(1, reps)):
+        t0 = time.perf_counter()
+        O.spmm_f32(0, nr, A.nc, rp, ci, va, B, nv)
+        times.append((time.perf_counter() - t0) * 1e3)
+    return statistics.median(times), nnz, nr, "port", 1
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args):
+    import numpy as np
+    import daspmm as D
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    A = D.gen_powerlaw(NR, seed=0)
+    B = D.gen_dense(A.nc * NV, seed=1)
+    threads = os.cpu_count() or 1
+    # calibrate: one full pass, then a row sample sized so W+K steps take ~60 s
+    full_ms, _, _, kind, _ = cpu_reference_time(A, B, NV, threads, 1)
+    budget_ms = 60e3 / max(1, args.steps + args.warmup)
+    rows = NR if full_ms <= budget_ms else max(1024, int(NR * budget_ms / full_ms))
+    for _ in range(args.warmup):
+        cpu_reference_time(A, B, NV, threads, 1, rows)
+    times = []
+    nnz_s = None
+    for _ in range(args.steps):
+        ms, nnz_s, nr_s, kind, cores = cpu_reference_time(A, B, NV, threads, 1, rows)
+        times.append(ms)
+    ms = statistics.median(times)
+    gflops = 2.0 * nnz_s * NV / (ms * 1e-3) / 1e9
+    sample = (f"rows 0..{rows - 1} of the 262144-row matrix ({nnz_s} nnz, N=128), one pass "
+              f"per step on {cores} threads (row slices), median of {args.steps}")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(gflops, 3), "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": workload_name("cpuSpmvReference (host)"), "nr": NR, "nv": NV,
+                   "nnz": A.nnz},
+        "cpu_baseline": {"value": round(gflops, 3), "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": round(gflops, 3), "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args):
+    import numpy as np
+    import torch
+    import daspmm as D
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+        pg = dist
+    L = D.lib()
+    alg = D.Alg[args.alg]
+
+    A = D.gen_powerlaw(NR, seed=rank)           # this rank's row shard
+    B = D.gen_dense(A.nc * NV, seed=1)          # B replicated on every rank
+    dA = D.DeviceCsr(A, dev)
+    Bt = torch.from_numpy(B).to(dev)
+    Ct = torch.zeros(A.nr * NV, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    cfg = D.default_config(alg, 0, A.nr, A.nc, A.nnz, NV) if alg != D.Alg.AUTO else None
+
+    def step():
+        D.spmm(alg, 0, dA, Bt, Ct, beta=0.0, nv=NV, stream=stream, cfg=None)
+
+    # warm-up steps, then a ~1.5 s burst so clocks settle (both untimed)
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize(dev)
+    gpu_uuid = None
+    try:
+        gpu_uuid = str(torch.cuda.get_device_properties(dev).uuid)
+        if not gpu_uuid.startswith("GPU-"):
+            gpu_uuid = "GPU-" + gpu_uuid
+    except Exception:
+        gpu_uuid = None
+    sampler = ClockSampler(gpu_uuid)
+    sampler.start()
+    t_burst = time.time()
+    while time.time() - t_burst < 1.5:
+        for _ in range(200):
+            step()
+        torch.cuda.synchronize(dev)
+
+    # main-kernel event ring for the timed region
+    K = args.steps
+    ev_s = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    ev_e = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    arr_s = (ctypes.c_void_p * K)(*[e.cuda_event for e in ev_s])
+    arr_e = (ctypes.c_void_p * K)(*[e.cuda_event for e in ev_e])
+    for e in ev_s + ev_e:   # materialise the events on this device
+        e.record(stream)
+    torch.cuda.synchronize(dev)
+    L.daspmm_set_kernel_timer(arr_s, arr_e, K)
+
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize(dev)
+    launches0 = L.daspmm_launch_count()
+    t0 = time.time()
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(K):
+        step()
+    stop.record(stream)
+    torch.cuda.synchronize(dev)
+    t1 = time.time()
+    if pg:
+        pg.barrier()
+    launches = L.daspmm_launch_count() - launches0
+    L.daspmm_set_kernel_timer(None, None, 0)
+    sampler.stop()
+
+    ms_total = start.elapsed_time(stop)
+    kern_ms = sum(s.elapsed_time(e) for s, e in zip(ev_s, ev_e)) / K
+    nnz_total = A.nnz
+    if pg:
+        t = torch.tensor([ms_total, kern_ms], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms_total, kern_ms = float(t[0]), float(t[1])
+        n = torch.tensor([A.nnz], dtype=torch.float64, device=dev)
+        pg.all_reduce(n, op=pg.ReduceOp.SUM)
+        nnz_total = int(n.item())
+    ms_step = ms_total / K
+    gflops = 2.0 * nnz_total * NV * K / (ms_total * 1e-3) / 1e9
+
+    # roofline of the main kernel (rank 0's shard shape)
+    abytes = algorithmic_bytes(A, NV)
+    peak, peak_src = measured_peak()
+    achieved = abytes / (kern_ms * 1e-3) / 1e9
+    traffic = None
+    tr = committed_traffic()
+    if tr and tr.get("nnz") == A.nnz:
+        traffic = tr.get("dram_bytes_per_launch")
+
+    line = None
+    if rank == 0:
+        # CPU baseline: the reference's host loop, 1 thread (it is serial), full matrix
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            ms_cpu, nnz_s, _, kind, cores = cpu_reference_time(A, B, NV, 1, 3)
+            cpu = {"value": round(2.0 * nnz_s * NV / (ms_cpu * 1e-3) / 1e9, 3), "unit": UNIT,
+                   "cores": cores, "kind": kind,
+                   "sample": f"full matrix ({nnz_s} nnz, N=128), median of 3 passes, 1 thread"}
+        # end to end through the host-buffer entry point
+        e2e = None
+        if not args.no_e2e:
+            e2e = run_e2e(D, A, B, dev, alg, min(K, args.e2e_steps))
+        clk = sampler.summary()
+        clk_in = sampler.summary(t0, t1)
+        clocks = {"sm_mhz": clk_in["sm_mhz"] if clk_in["samples"] else clk["sm_mhz"],
+                  "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
+                  "samples_timed": clk_in["samples"], "samples_total": clk["samples"],
+                  "window": "200 ms nvidia-smi samples over a 1.5 s burst of the same step "
+                            "right before the timed region and the timed region itself"}
+        cfg_used = D.default_config(alg, 0, A.nr, A.nc, A.nnz, NV)
+        line = {
+            "metric": METRIC, "value": round(gflops, 3), "unit": UNIT, "n_gpus": world,
+            "steps": K, "warmup": args.warmup, "ms_per_step": round(ms_step, 5),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": workload_name(alg.name), "nr": A.nr, "nnz": A.nnz, "nv": NV,
+                       "variant": cfg_used.as_dict(),
+                       "l2": "inputs larger than L2 (working set %.0f MB > 126 MB), no flush"
+                             % (abytes / 1e6),
+                       "parallelism": f"row shards x{world}, B replicated, no collective"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "traffic": traffic, "kernel": "k_bal (main gather kernel)",
+                         "kernel_ms": round(kern_ms, 5), "algorithmic_bytes": abytes,
+                         "peak_source": peak_src},
+            "step_hbm_gbs": round(abytes / (ms_step * 1e-3) / 1e9, 1),
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": int(launches),
+        }
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_e2e(D, A, B, dev, alg, steps):
+    """Same SpMM through daspmm_spmm_host: pinned host A, B in; C out."""
+    import numpy as np
+    import torch
+    L = D.lib()
+    pin = lambda a: torch.from_numpy(a).pin_memory()
+    rp, ci, va, Bh = pin(A.rowPtr), pin(A.colIdx), pin(A.values), pin(B)
+    Ch = torch.empty(A.nr * NV, dtype=torch.float32).pin_memory()
+    cfg = D.default_config(alg, 0, A.nr, A.nc, A.nnz, NV)
+    stream = torch.cuda.current_stream(dev)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+
+    def once():
+        D.check(L.daspmm_spmm_host(ctypes.byref(cfg), 0, A.nr, A.nc, A.nnz, NV,
+                                   ctypes.c_void_p(rp.data_ptr()), None,
+                                   ctypes.c_void_p(ci.data_ptr()), ctypes.c_void_p(va.data_ptr()),
+                                   ctypes.c_void_p(Bh.data_ptr()), ctypes.c_void_p(Ch.data_ptr()),
+                                   0.0, sp), "spmm_host")
+    once()
+    once()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        once()
+    dt = (time.perf_counter() - t0) / steps
+    h2d = 4 * (A.nr + 1) + 8 * A.nnz + 4 * A.nc * NV
+    d2h = 4 * A.nr * NV
+    return {"value": round(2.0 * A.nnz * NV / dt / 1e9, 3), "unit": UNIT,
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "ms_per_step": round(dt * 1e3, 4), "steps": steps,
+            "path": "daspmm_spmm_host: pinned host rowPtr/colIdx/values/B -> device, SpMM, "
+                    "C -> pinned host, stream synchronised each step"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--alg", default="CSR_BALANCED",
+                    choices=["CSR_SCALAR", "CSR_VECTOR", "COO_SCALAR", "COO_VECTOR",
+                             "CSR_BALANCED", "AUTO"])
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

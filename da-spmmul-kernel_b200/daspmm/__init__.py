@@ -1,0 +1,340 @@
+"""Python bindings of libdaspmm.so (the C ABI in include/daspmm.h).
+
+ctypes over the shared library; torch tensors supply device memory and
+streams only.  Loading fails loudly when the library has not been built --
+there is no CPU fallback for any computation here.
+
+Mirrors the reference's host interface (ASPLOS-2022/DA-SpMMul-kernel):
+``SPMV_SPMM_ALG`` (spmvspmm.h:5-10), ``DenseLayout`` (helper.h:261-264),
+``SpmvSpmmProblem`` (spmvspmm.h:13-50, 202-273) and ``cudaSpmm``
+(spmvspmm.h:53-199).
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "libdaspmm.so")
+
+
+class DaspmmError(RuntimeError):
+    """A libdaspmm call returned a non-zero status."""
+
+    def __init__(self, status: int, what: str = ""):
+        self.status = int(status)
+        msg = _lib().daspmm_status_string(int(status)).decode()
+        if self.status == 3:
+            msg += f" (cudaError {_lib().daspmm_last_cuda_error()})"
+        super().__init__(f"{what}: {msg}" if what else msg)
+
+
+class Alg(enum.IntEnum):
+    """SPMV_SPMM_ALG (spmvspmm.h:5-10) plus this library's extensions."""
+
+    CSR_SCALAR = 0
+    CSR_VECTOR = 1
+    COO_SCALAR = 2
+    COO_VECTOR = 3
+    CSR_BALANCED = 4
+    AUTO = 5
+
+
+class Layout(enum.IntEnum):
+    """DenseLayout (helper.h:261-264)."""
+
+    ROW_MAJOR = 0
+    COL_MAJOR = 1
+
+
+class Fmt(enum.IntEnum):
+    F32 = 0
+    BF16 = 1
+    F16 = 2
+    E4M3 = 3
+
+
+class Config(ctypes.Structure):
+    """daspmm_config: one point of the design space (0 = library default)."""
+
+    _fields_ = [(n, ctypes.c_int) for n in
+                ("alg", "vec", "lanes_col", "lanes_nnz", "cf", "chunk", "snap", "block")]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+    def __repr__(self):
+        return "Config(" + ", ".join(f"{k}={v}" for k, v in self.as_dict().items()) + ")"
+
+
+_LIB = None
+_VP = ctypes.c_void_p
+_I = ctypes.c_int
+
+
+def _lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `make -C {os.path.dirname(_HERE)}` "
+                "(or __graft_entry__.build()); there is no fallback implementation")
+        lib = ctypes.CDLL(LIB_PATH)
+        sig = {
+            "daspmm_spmm": (_I, [_I, _I, _I, _I, _I, _I, _VP, _VP, _VP, _VP, _VP, _VP,
+                                 ctypes.c_float, _VP]),
+            "daspmm_spmm_ex": (_I, [ctypes.POINTER(Config), _I, _I, _I, _I, _I, _VP, _VP, _VP,
+                                    _VP, _VP, _VP, ctypes.c_float, _VP, ctypes.c_size_t, _VP]),
+            "daspmm_workspace_bytes": (ctypes.c_size_t,
+                                       [ctypes.POINTER(Config), _I, _I, _I, _I]),
+            "daspmm_default_config": (_I, [_I, _I, _I, _I, _I, _I, ctypes.POINTER(Config)]),
+            "daspmm_compat_spmm": (_I, [_I, _I, _I, _I, _I, _I, _VP, _VP, _VP, _VP, _VP, _VP]),
+            "daspmm_num_chunks": (_I, [_I, _I]),
+            "daspmm_partition": (_I, [_I, _I, _VP, _I, _I, _VP, _VP]),
+            "daspmm_ownership": (_I, [_I, _I, _I, _VP, _VP, _I, _I, _VP, _VP]),
+            "daspmm_coo_to_csr": (_I, [_I, _I, _VP, _VP, _VP]),
+            "daspmm_status_string": (ctypes.c_char_p, [_I]),
+            "daspmm_last_cuda_error": (_I, []),
+            "daspmm_abi_version": (_I, []),
+            "daspmm_gen_uniform": (_I, [_I, _I, _I, ctypes.c_uint64, _VP, _VP, _VP]),
+            "daspmm_gen_powerlaw": (_I, [_I, _I, ctypes.c_double, ctypes.c_double, _I, _I,
+                                         ctypes.c_double, ctypes.c_uint64, _VP, _VP, _VP,
+                                         ctypes.POINTER(ctypes.c_longlong)]),
+            "daspmm_gen_random": (_I, [_I, _I, ctypes.c_double, ctypes.c_uint64, _VP, _VP, _VP,
+                                       ctypes.POINTER(ctypes.c_longlong)]),
+            "daspmm_gen_dense": (None, [ctypes.c_size_t, ctypes.c_uint64, ctypes.c_float,
+                                        ctypes.c_float, _VP]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _extend_signatures(lib)
+        _LIB = lib
+    return _LIB
+
+
+def _extend_signatures(lib):
+    """Signatures of entry points added by later modules of the library."""
+    from . import _sigs
+    _sigs.apply(lib, Config)
+
+
+def lib():
+    """The loaded libdaspmm.so (ctypes.CDLL)."""
+    return _lib()
+
+
+def check(status: int, what: str = "") -> None:
+    if status != 0:
+        raise DaspmmError(status, what)
+
+
+def _np_ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+# ---------------------------------------------------------------- matrices
+@dataclass
+class Csr:
+    """Host CSR matrix (int32 indices, float32 values), sorted by (row, col)."""
+
+    nr: int
+    nc: int
+    rowPtr: np.ndarray
+    colIdx: np.ndarray
+    values: np.ndarray
+
+    @property
+    def nnz(self) -> int:
+        return int(self.rowPtr[-1]) if self.nr > 0 else 0
+
+    @property
+    def rowIdx(self) -> np.ndarray:
+        """COO row indices (the reference driver passes both, spmvspmm_benchmark.cu:370)."""
+        return np.repeat(np.arange(self.nr, dtype=np.int32), np.diff(self.rowPtr)).astype(np.int32)
+
+    def cols_touched(self) -> int:
+        return int(np.unique(self.colIdx).size) if self.nnz else 0
+
+
+def gen_uniform(nr: int, nc: int, per_row: int, seed: int = 0) -> Csr:
+    """Exactly per_row distinct uniform columns per row, values U(-1,1)."""
+    L = _lib()
+    rp = np.zeros(nr + 1, np.int32)
+    ci = np.zeros(max(1, nr * per_row), np.int32)
+    va = np.zeros(max(1, nr * per_row), np.float32)
+    check(L.daspmm_gen_uniform(nr, nc, per_row, seed, _np_ptr(rp), _np_ptr(ci), _np_ptr(va)),
+          "gen_uniform")
+    n = nr * per_row
+    return Csr(nr, nc, rp, ci[:n].copy(), va[:n].copy())
+
+
+def gen_powerlaw(n: int, alpha: float = 2.1, shift: float = 0.16, dmin: int = 1,
+                 dmax: int = 4096, seed: int = 0, mean_scale: float = 1.0,
+                 nc: int | None = None) -> Csr:
+    """Power-law out-degrees, preferential-attachment columns, values U(-1,1)."""
+    L = _lib()
+    nc = n if nc is None else nc
+    rp = np.zeros(n + 1, np.int32)
+    nnz = ctypes.c_longlong(0)
+    check(L.daspmm_gen_powerlaw(n, nc, alpha, shift, dmin, dmax, mean_scale, seed,
+                                _np_ptr(rp), None, None, ctypes.byref(nnz)), "gen_powerlaw")
+    ci = np.zeros(max(1, nnz.value), np.int32)
+    va = np.zeros(max(1, nnz.value), np.float32)
+    check(L.daspmm_gen_powerlaw(n, nc, alpha, shift, dmin, dmax, mean_scale, seed,
+                                _np_ptr(rp), _np_ptr(ci), _np_ptr(va), ctypes.byref(nnz)),
+          "gen_powerlaw")
+    return Csr(n, nc, rp, ci[:nnz.value].copy(), va[:nnz.value].copy())
+
+
+def gen_random(nr: int, nc: int, avg_deg: float, seed: int = 0) -> Csr:
+    """Poisson(avg_deg) distinct uniform columns per row, values U(-1,1)."""
+    L = _lib()
+    rp = np.zeros(nr + 1, np.int32)
+    nnz = ctypes.c_longlong(0)
+    check(L.daspmm_gen_random(nr, nc, avg_deg, seed, _np_ptr(rp), None, None,
+                              ctypes.byref(nnz)), "gen_random")
+    ci = np.zeros(max(1, nnz.value), np.int32)
+    va = np.zeros(max(1, nnz.value), np.float32)
+    check(L.daspmm_gen_random(nr, nc, avg_deg, seed, _np_ptr(rp), _np_ptr(ci), _np_ptr(va),
+                              ctypes.byref(nnz)), "gen_random")
+    return Csr(nr, nc, rp, ci[:nnz.value].copy(), va[:nnz.value].copy())
+
+
+def gen_dense(n: int, seed: int = 1, lo: float = -1.0, hi: float = 1.0) -> np.ndarray:
+    out = np.empty(max(1, n), np.float32)
+    _lib().daspmm_gen_dense(n, seed, lo, hi, _np_ptr(out))
+    return out[:n]
+
+
+def default_config(alg: int, layout: int, nr: int, nc: int, nnz: int, nv: int) -> Config:
+    c = Config()
+    check(_lib().daspmm_default_config(int(alg), int(layout), nr, nc, nnz, nv, ctypes.byref(c)),
+          "default_config")
+    return c
+
+
+def num_chunks(nnz: int, chunk: int) -> int:
+    return _lib().daspmm_num_chunks(nnz, chunk)
+
+
+def workspace_bytes(cfg: Config, layout: int, nr: int, nnz: int, nv: int) -> int:
+    return _lib().daspmm_workspace_bytes(ctypes.byref(cfg), int(layout), nr, nnz, nv)
+
+
+# ---------------------------------------------------------------- device side
+def _dptr(t):
+    """Device address of a torch tensor (None -> NULL)."""
+    if t is None:
+        return None
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        return None
+    return ctypes.c_void_p(getattr(stream, "cuda_stream", stream))
+
+
+class DeviceCsr:
+    """A CSR/COO matrix resident in device memory (torch tensors)."""
+
+    def __init__(self, A: Csr, device="cuda"):
+        import torch
+        self.nr, self.nc, self.nnz = A.nr, A.nc, A.nnz
+        self.rowPtr = torch.from_numpy(A.rowPtr).to(device)
+        self.rowIdx = torch.from_numpy(A.rowIdx).to(device)
+        self.colIdx = torch.from_numpy(A.colIdx).to(device)
+        self.values = torch.from_numpy(A.values).to(device)
+
+
+def spmm(alg: int, layout: int, A: DeviceCsr, B, C, beta: float = 0.0, nv: int | None = None,
+         stream=None, cfg: Config | None = None, workspace=None) -> None:
+    """C = A*B + beta*C on the device (libdaspmm.daspmm_spmm / daspmm_spmm_ex)."""
+    L = _lib()
+    if nv is None:
+        nv = B.shape[1] if (layout == Layout.ROW_MAJOR and B.dim() == 2) else (
+            B.shape[0] if B.dim() == 2 else 1)
+    if cfg is None:
+        st = L.daspmm_spmm(int(alg), int(layout), A.nr, A.nc, A.nnz, nv, _dptr(A.rowPtr),
+                           _dptr(A.rowIdx), _dptr(A.colIdx), _dptr(A.values), _dptr(B), _dptr(C),
+                           float(beta), _stream_ptr(stream))
+    else:
+        ws = _dptr(workspace)
+        wsb = workspace.numel() * workspace.element_size() if workspace is not None else 0
+        st = L.daspmm_spmm_ex(ctypes.byref(cfg), int(layout), A.nr, A.nc, A.nnz, nv,
+                              _dptr(A.rowPtr), _dptr(A.rowIdx), _dptr(A.colIdx), _dptr(A.values),
+                              _dptr(B), _dptr(C), float(beta), ws, wsb, _stream_ptr(stream))
+    check(st, "daspmm_spmm")
+
+
+def compat_spmm(alg: int, layout: int, A: DeviceCsr, B, C, nv: int) -> int:
+    """cudaSpmm<256,32> semantics (CSR overwrite, COO accumulate); returns cudaError_t."""
+    return _lib().daspmm_compat_spmm(int(alg), int(layout), A.nr, A.nc, A.nnz, nv,
+                                     _dptr(A.rowPtr), _dptr(A.rowIdx), _dptr(A.colIdx),
+                                     _dptr(A.values), _dptr(B), _dptr(C))
+
+
+def partition(A: DeviceCsr, chunk: int, snap: int, stream=None):
+    import torch
+    n = num_chunks(A.nnz, chunk)
+    meta = torch.empty(2 * (n + 1), dtype=torch.int32, device=A.rowPtr.device)
+    check(_lib().daspmm_partition(A.nr, A.nnz, _dptr(A.rowPtr), chunk, snap, _dptr(meta),
+                                  _stream_ptr(stream)), "partition")
+    return meta
+
+
+def ownership(alg: int, A: DeviceCsr, chunk: int, snap: int = 1, stream=None):
+    import torch
+    own = torch.empty(2 * max(1, A.nr), dtype=torch.int32, device=A.rowPtr.device)
+    check(_lib().daspmm_ownership(int(alg), A.nr, A.nnz, _dptr(A.rowPtr), _dptr(A.rowIdx),
+                                  chunk, snap, _dptr(own), _stream_ptr(stream)), "ownership")
+    return own[: 2 * A.nr]
+
+
+def coo_to_csr(nr: int, rowIdx, stream=None):
+    import torch
+    rp = torch.empty(nr + 1, dtype=torch.int32, device=rowIdx.device)
+    check(_lib().daspmm_coo_to_csr(nr, rowIdx.numel(), _dptr(rowIdx), _dptr(rp),
+                                   _stream_ptr(stream)), "coo_to_csr")
+    return rp
+
+
+# ---------------------------------------------------------------- problem
+class SpmvSpmmProblem:
+    """Non-owning view of device buffers with run/benchmark, after
+    SpmvSpmmProblem (spmvspmm.h:13-50, 202-243).  `run` keeps the reference's
+    power-of-two check and its print-and-return behaviour for bad nv."""
+
+    def __init__(self, A: DeviceCsr, dnInput, dnOutput, maxNv: int):
+        self.A, self.dnInput, self.dnOutput, self.maxNv = A, dnInput, dnOutput, maxNv
+
+    def run(self, layout: int, nv: int, alg: int) -> None:
+        if nv & (nv - 1):
+            import sys
+            print(f"nv must be power of 2, less than 32. Got nv = {nv}", file=sys.stderr)
+            return
+        err = compat_spmm(alg, layout, self.A, self.dnInput, self.dnOutput, nv)
+        if err != 0:
+            raise DaspmmError(3, f"cudaSpmm returned cudaError {err}")
+
+    def benchmark(self, layout: int, nv: int, alg: int, warmupIters: int = 5,
+                  repeatIters: int = 50) -> float:
+        import torch
+        if nv & (nv - 1):
+            return -1.0
+        for _ in range(warmupIters):
+            compat_spmm(alg, layout, self.A, self.dnInput, self.dnOutput, nv)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(torch.cuda.default_stream())
+        for _ in range(repeatIters):
+            compat_spmm(alg, layout, self.A, self.dnInput, self.dnOutput, nv)
+        e.record(torch.cuda.default_stream())
+        e.synchronize()
+        return s.elapsed_time(e) / repeatIters

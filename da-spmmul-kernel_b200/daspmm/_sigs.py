@@ -1,0 +1,24 @@
+"""ctypes signatures of entry points beyond the core FP32 path.
+
+Kept separate so each added part of the C ABI declares its own signatures in
+one place; `apply` skips names the loaded library does not export.
+"""
+import ctypes
+
+_VP = ctypes.c_void_p
+_I = ctypes.c_int
+
+
+def apply(lib, Config):
+    sig = {
+        "daspmm_spmm_host": (_I, [ctypes.POINTER(Config), _I, _I, _I, _I, _I, _VP, _VP, _VP,
+                                  _VP, _VP, _VP, ctypes.c_float, _VP]),
+        "daspmm_launch_count": (ctypes.c_longlong, []),
+        "daspmm_set_kernel_timer": (None, [ctypes.POINTER(_VP), ctypes.POINTER(_VP), _I]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name, None)
+        if f is None:
+            continue
+        f.restype = res
+        f.argtypes = args

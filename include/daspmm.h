@@ -1,0 +1,209 @@
+/*
+ * daspmm.h -- C ABI of the B200 (sm_100a) SpMM/SpMV library libdaspmm.so.
+ *
+ * Plain C: pointers, sizes and status codes; no CUDA or C++ types.  Device
+ * pointers are raw CUDA device addresses owned by the caller; `stream` is a
+ * cudaStream_t passed as void* (NULL = the legacy default stream, which is
+ * what the reference uses for every launch, helper.h:176,181).
+ *
+ * Sparse matrix A: nr x nc with nnz nonzeros, int32 indices, sorted by
+ * (row, col).  CSR algorithms read rowPtr[nr+1]; COO algorithms read
+ * rowIdx[nnz]; both read colIdx[nnz] and values[nnz] (the reference's driver
+ * supplies both arrays over the same colIdx/values,
+ * spmvspmm_benchmark.cu:367-376).  Dense B is nc x nv and C is nr x nv, both
+ * row-major (B[col*nv+k]) or both col-major (B[k*nc+col]), as in
+ * spmm.h:296-310.
+ *
+ * No function here exits the process or prints; every failure is a status.
+ */
+#ifndef DASPMM_H
+#define DASPMM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define DASPMM_ABI_VERSION 1
+
+typedef enum daspmm_status {
+    DASPMM_OK = 0,
+    DASPMM_ERR_INVALID = 1,      /* bad argument: sizes, null pointer, layout, nv */
+    DASPMM_ERR_UNSUPPORTED = 2,  /* combination of algorithm/layout/config not provided */
+    DASPMM_ERR_CUDA = 3,         /* a CUDA call failed; see daspmm_last_cuda_error() */
+    DASPMM_ERR_NOMEM = 4,        /* device allocation failed */
+    DASPMM_ERR_WORKSPACE = 5,    /* caller workspace smaller than required */
+    DASPMM_ERR_TIMEOUT = 6,      /* a bounded wait expired */
+    DASPMM_ERR_BUDGET = 7,       /* request exceeds the memory budget (serving) */
+    DASPMM_ERR_CANCELLED = 8,    /* request cancelled (serving) */
+    DASPMM_ERR_BAD_MATRIX = 9    /* validation failed: rowPtr/rowIdx/colIdx malformed */
+} daspmm_status;
+
+/* Algorithm ids 0..3 have the values of enum SPMV_SPMM_ALG
+ * (spmvspmm.h:5-10) and the reference's semantics: CSR algorithms overwrite C
+ * (C = A*B), COO algorithms accumulate (C += A*B) -- see beta below. */
+enum {
+    DASPMM_ALG_CSR_SCALAR = 0,   /* row-balanced, sequential reduction   (SR_RB) */
+    DASPMM_ALG_CSR_VECTOR = 1,   /* row-balanced, warp-parallel reduction (PR_RB) */
+    DASPMM_ALG_COO_SCALAR = 2,   /* nonzero-balanced, sequential          (SR_EB) */
+    DASPMM_ALG_COO_VECTOR = 3,   /* nonzero-balanced, segmented parallel   (PR_EB) */
+    DASPMM_ALG_CSR_BALANCED = 4, /* nonzero-balanced over CSR with short-row snapping */
+    DASPMM_ALG_AUTO = 5          /* autotuned choice among the above (CSR semantics) */
+};
+
+/* Dense layouts: values of enum DenseLayout (helper.h:261-264). */
+enum { DASPMM_ROW_MAJOR = 0, DASPMM_COL_MAJOR = 1 };
+
+/* Storage formats for the mixed-precision entry points. */
+enum { DASPMM_F32 = 0, DASPMM_BF16 = 1, DASPMM_F16 = 2, DASPMM_E4M3 = 3 };
+
+/* A point of the design space.  Zero fields take the library default for the
+ * problem shape. */
+typedef struct daspmm_config {
+    int alg;        /* DASPMM_ALG_* (0..4) */
+    int vec;        /* floats per vector access: 1, 2 or 4 (16-byte loads) */
+    int lanes_col;  /* L: lanes splitting the dense columns (power of two <= 32) */
+    int lanes_nnz;  /* S: lanes splitting the nonzeros (power of two, L*S <= 32) */
+    int cf;         /* column-coarsening factor: vectors per lane (1, 2; CM 1..8) */
+    int chunk;      /* nonzeros per chunk for the nonzero-balanced splits */
+    int snap;       /* balanced CSR: rows shorter than this are never split */
+    int block;      /* threads per CTA: 128 or 256 */
+} daspmm_config;
+
+/* ---- FP32 SpMM ---------------------------------------------------------
+ * C = A*B + beta*C.  beta == 0 never reads C.  For the COO algorithms a beta
+ * other than 1 first scales all of C (rows without nonzeros included).
+ * Uses a workspace the library keeps per (device, stream); the call that first
+ * needs a larger one synchronises the stream and allocates (so it must not be
+ * the first call inside a stream capture).
+ * Replaces: cudaSpmm<kBlockSize,kWarpSize>(alg, layout, nr, nc, nnz, nv,
+ * rowPtr, rowIdx, colIdx, values, dnInput, dnOutput) (spmvspmm.h:53-199),
+ * which has beta fixed by the algorithm. */
+daspmm_status daspmm_spmm(int alg, int layout, int nr, int nc, int nnz, int nv,
+                          const int *rowPtr, const int *rowIdx, const int *colIdx,
+                          const float *values, const float *B, float *C,
+                          float beta, void *stream);
+
+/* Same with an explicit design-space point and caller-owned workspace of
+ * ws_bytes (>= daspmm_workspace_bytes(...)); workspace == NULL falls back to
+ * the library's per-stream workspace.  No counterpart in the reference (its
+ * template parameters kBlockSize/kWarpSize are fixed at 256/32). */
+daspmm_status daspmm_spmm_ex(const daspmm_config *cfg, int layout, int nr, int nc,
+                             int nnz, int nv, const int *rowPtr, const int *rowIdx,
+                             const int *colIdx, const float *values, const float *B,
+                             float *C, float beta, void *workspace, size_t ws_bytes,
+                             void *stream);
+
+/* Workspace bytes daspmm_spmm_ex needs for this configuration and shape. */
+size_t daspmm_workspace_bytes(const daspmm_config *cfg, int layout, int nr, int nnz,
+                              int nv);
+
+/* Fill *out with the configuration the library would use for this shape
+ * (the defaults; or the autotuner's cached choice for DASPMM_ALG_AUTO once
+ * daspmm_autotune has run for the fingerprint). */
+daspmm_status daspmm_default_config(int alg, int layout, int nr, int nc, int nnz,
+                                    int nv, daspmm_config *out);
+
+/* ---- Drop-in for the reference's dispatcher ------------------------------
+ * Exactly cudaSpmm<256,32> (spmvspmm.h:53-199): CSR algorithms overwrite C,
+ * COO algorithms add into C, the legacy default stream, and the return value
+ * is a cudaError_t (0 = cudaSuccess; cudaErrorInvalidValue = 1 for bad
+ * arguments).  Any nv >= 1 is accepted (the reference's power-of-two check
+ * lives in SpmvSpmmProblem::run, spmvspmm.h:209). */
+int daspmm_compat_spmm(int alg, int layout, int nr, int nc, int nnz, int nv,
+                       const int *rowPtr, const int *rowIdx, const int *colIdx,
+                       const float *values, const float *dnInput, float *dnOutput);
+
+/* ---- Partition tables (bit-exact contract; used by tests) ----------------
+ * Number of chunks for a nonzero-balanced split: max(1, ceil(nnz/chunk)). */
+int daspmm_num_chunks(int nnz, int chunk);
+
+/* Balanced-CSR boundaries on the device: meta[2c] = first nonzero of chunk c
+ * after snapping, meta[2c+1] = its row; nchunks+1 entries (int pairs).
+ * No reference counterpart (helper.h:283-321 has only a commented-out
+ * binary_search_segment_number). */
+daspmm_status daspmm_partition(int nr, int nnz, const int *rowPtr, int chunk,
+                               int snap, int *meta, void *stream);
+
+/* Output-row ownership the kernels realise: for each row r, owner[2r] = chunk
+ * that writes it (or -1), owner[2r+1] = number of chunks holding a piece of
+ * it.  alg = DASPMM_ALG_CSR_BALANCED (uses rowPtr) or DASPMM_ALG_COO_SCALAR
+ * (uses rowIdx).  owner is device memory of 2*nr ints.  Runs the kernels'
+ * own traversal with the arithmetic switched off. */
+daspmm_status daspmm_ownership(int alg, int nr, int nnz, const int *rowPtr,
+                               const int *rowIdx, int chunk, int snap, int *owner,
+                               void *stream);
+
+/* ---- Format conversion -----------------------------------------------------
+ * Device COO -> CSR row pointer from sorted rowIdx[nnz]; rowPtr has nr+1
+ * entries.  Bit-exact with generateCsrRowPtrArray
+ * (spmvspmm_benchmark.cu:41-76), and defined for nnz == 0. */
+daspmm_status daspmm_coo_to_csr(int nr, int nnz, const int *rowIdx, int *rowPtr,
+                                void *stream);
+
+/* ---- Host buffers ------------------------------------------------------
+ * The same product with A, B and C in HOST memory (pinned or pageable): the
+ * library copies A and B to device buffers it keeps per (device, stream),
+ * runs daspmm_spmm_ex, copies C back and synchronises the stream before it
+ * returns.  C is read (copied in) only when beta != 0.  rowIdx may be NULL
+ * for CSR algorithms and rowPtr NULL for COO algorithms.  The entry point
+ * of a caller that holds its matrices on the host (the reference's driver
+ * copies them itself, spmvspmm_benchmark.cu:369-383). */
+daspmm_status daspmm_spmm_host(const daspmm_config *cfg, int layout, int nr, int nc,
+                               int nnz, int nv, const int *rowPtr, const int *rowIdx,
+                               const int *colIdx, const float *values, const float *B,
+                               float *C, float beta, void *stream);
+
+/* ---- Diagnostics ------------------------------------------------------- */
+/* Number of kernels this library has launched in this process. */
+long long daspmm_launch_count(void);
+
+/* Kernel timing hook: while n > 0, every SpMM call records start_events[i]
+ * immediately before and stop_events[i] immediately after the launch of its
+ * main (gather) kernel, on the call's stream, with i cycling 0..n-1 (events
+ * are cudaEvent_t passed as void*).  n = 0 switches it off.  Process-wide;
+ * meant for benchmarks. */
+void daspmm_set_kernel_timer(void **start_events, void **stop_events, int n);
+
+const char *daspmm_status_string(daspmm_status s);
+int daspmm_last_cuda_error(void);   /* cudaError_t of the last failure on this thread */
+int daspmm_abi_version(void);
+
+/* ---- Host-side synthetic inputs (deterministic for a seed) -----------------
+ * Exactly `per_row` distinct uniformly random columns per row, sorted; values
+ * U(-1,1).  rowPtr[nr+1], colIdx/values[nr*per_row]. */
+daspmm_status daspmm_gen_uniform(int nr, int nc, int per_row, uint64_t seed,
+                                 int *rowPtr, int *colIdx, float *values);
+
+/* Power-law graph: out-degree k in [dmin, dmax] with p(k) ~ (k + shift)^-alpha,
+ * columns by preferential attachment (probability ~ in-degree + 1, duplicates
+ * in a row redrawn), values U(-1,1).  Two calls: first with colIdx == NULL to
+ * get rowPtr (returns nnz in *nnz_out), then with the arrays allocated.
+ * mean_scale != 1 multiplies every degree (rounded, clamped to [dmin, dmax]),
+ * for families with a target average degree. */
+daspmm_status daspmm_gen_powerlaw(int nr, int nc, double alpha, double shift,
+                                  int dmin, int dmax, double mean_scale,
+                                  uint64_t seed, int *rowPtr, int *colIdx,
+                                  float *values, long long *nnz_out);
+
+/* Uniform random sparse matrix with Poisson(avg_deg) distinct columns per row
+ * (two calls as above). */
+daspmm_status daspmm_gen_random(int nr, int nc, double avg_deg, uint64_t seed,
+                                int *rowPtr, int *colIdx, float *values,
+                                long long *nnz_out);
+
+/* n floats U(lo, hi). */
+void daspmm_gen_dense(size_t n, uint64_t seed, float lo, float hi, float *out);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#ifdef __cplusplus
+}
+#endif
+#endif /* DASPMM_H */

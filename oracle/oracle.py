@@ -1,0 +1,220 @@
+"""Python wrapper of the CPU oracle (liboracle.so) and, when built, of the
+harness around the unmodified reference (_ref/libref.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline / reference legs of bench.py, as the checker.  The product
+(libdaspmm.so and its bindings) never imports this module.
+
+Each function names the reference code it restates (see oracle.c).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "libref.so")
+
+_VP = ctypes.c_void_p
+_I = ctypes.c_int
+_lib = None
+_ref = None
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} missing: run `make -C {HERE} oracle`")
+        L = ctypes.CDLL(LIB_PATH)
+        sig = {
+            "or_coo_to_csr_rowptr": (_I, [_I, _I, _VP, _VP]),
+            "or_spmm_f32": (None, [_I, _I, _I, _I, _I, _VP, _VP, _VP, _VP, _VP]),
+            "or_spmm_f64": (None, [_I, _I, _I, _I, _I, _VP, _VP, _VP, _VP, _VP, _VP]),
+            "or_spmm_f64d": (None, [_I, _I, _I, _I, _I, _VP, _VP, _VP, _VP, _VP, _VP]),
+            "or_check_result": (_I, [_I, _I, _I, _I, _VP, _VP, ctypes.c_float, _I,
+                                     ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+            "or_calc_max_nv": (_I, [_I, _I, _I, ctypes.c_size_t, _I, _I]),
+            "or_row_of": (_I, [_VP, _I, _I]),
+            "or_num_chunks": (_I, [_I, _I]),
+            "or_balanced_partition": (None, [_I, _I, _VP, _I, _I, _VP]),
+            "or_balanced_ownership": (_I, [_I, _I, _VP, _I, _I, _VP]),
+            "or_coo_ownership": (_I, [_I, _I, _VP, _I, _VP]),
+            "or_quantize": (None, [_I, ctypes.c_size_t, _VP, _VP]),
+            "or_dequantize": (None, [_I, ctypes.c_size_t, _VP, _VP]),
+        }
+        for n, (r, a) in sig.items():
+            f = getattr(L, n)
+            f.restype, f.argtypes = r, a
+        _lib = L
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_PATH)
+
+
+def ref():
+    """The unmodified reference's host code and kernels (oracle/_ref/libref.so)."""
+    global _ref
+    if _ref is None:
+        if not ref_available():
+            raise ImportError(f"{REF_PATH} missing (built only where the reference tree exists)")
+        R = ctypes.CDLL(REF_PATH)
+        sig = {
+            "ref_cpu_spmm": (None, [_I, _I, _I, _I, _I, _VP, _VP, _VP, _VP, _VP]),
+            "ref_coo_to_csr": (_I, [_I, _I, _VP, _VP]),
+            "ref_check_result": (_I, [_I, _I, _I, _I, _VP, _VP, ctypes.c_float]),
+            "ref_cpu_bench": (ctypes.c_double, [_I, _I, _I, _I, _I, _VP, _VP, _VP, _VP, _I, _I]),
+            "ref_cuda_spmm": (_I, [_I, _I, _I, _I, _I, _I, _VP, _VP, _VP, _VP, _VP, _VP]),
+            "ref_cuda_bench": (ctypes.c_float, [_I, _I, _I, _I, _I, _I, _VP, _VP, _VP, _VP, _VP,
+                                                _VP, _I, _I]),
+            "ref_cusparse_bench": (ctypes.c_float, [_I, _I, _I, _I, _I, _I, _VP, _VP, _VP, _VP,
+                                                    _VP, _VP, _I, _I, _I]),
+        }
+        for n, (r, a) in sig.items():
+            f = getattr(R, n)
+            f.restype, f.argtypes = r, a
+        _ref = R
+    return _ref
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+# ---------------------------------------------------------------- oracle
+def coo_to_csr(nr: int, rowIdx) -> np.ndarray:
+    """generateCsrRowPtrArray (spmvspmm_benchmark.cu:41-76)."""
+    ri = _i32(rowIdx)
+    rp = np.zeros(nr + 1, np.int32)
+    if lib().or_coo_to_csr_rowptr(nr, ri.size, _p(ri), _p(rp)) != 0:
+        raise ValueError("rowIdx not sorted or out of range")
+    return rp
+
+
+def spmm_f32(layout: int, nr: int, nc: int, rowPtr, colIdx, values, B, nv: int) -> np.ndarray:
+    """cpuSpmvReference (spmvspmm_benchmark.cu:11-39); returns C flat in `layout`."""
+    rp, ci, va, b = _i32(rowPtr), _i32(colIdx), _f32(values), _f32(B).reshape(-1)
+    C = np.zeros(nr * nv, np.float32)
+    lib().or_spmm_f32(int(layout), nr, nc, int(rp[-1]) if nr else 0, nv, _p(rp), _p(ci), _p(va),
+                      _p(b), _p(C))
+    return C
+
+
+def spmm_f64(layout: int, nr: int, nc: int, rowPtr, colIdx, values, B, nv: int):
+    """FP64 product and the condition scale sum|a||b| per output element."""
+    rp, ci, va, b = _i32(rowPtr), _i32(colIdx), _f32(values), _f32(B).reshape(-1)
+    C = np.zeros(nr * nv, np.float64)
+    A = np.zeros(nr * nv, np.float64)
+    lib().or_spmm_f64(int(layout), nr, nc, int(rp[-1]) if nr else 0, nv, _p(rp), _p(ci), _p(va),
+                      _p(b), _p(C), _p(A))
+    return C, A
+
+
+def spmm_f64d(layout: int, nr: int, nc: int, rowPtr, colIdx, values64, B64, nv: int):
+    rp, ci = _i32(rowPtr), _i32(colIdx)
+    va = np.ascontiguousarray(values64, np.float64)
+    b = np.ascontiguousarray(B64, np.float64).reshape(-1)
+    C = np.zeros(nr * nv, np.float64)
+    A = np.zeros(nr * nv, np.float64)
+    lib().or_spmm_f64d(int(layout), nr, nc, int(rp[-1]) if nr else 0, nv, _p(rp), _p(ci), _p(va),
+                       _p(b), _p(C), _p(A))
+    return C, A
+
+
+def check_result(host_layout: int, dev_layout: int, nrows: int, ncols: int, ref, out,
+                 eps: float = 1e-3, first_only: bool = True):
+    """checkResult (spmvspmm_benchmark.cu:93-116): (passed, first_bad_(i, j))."""
+    r, o = _f32(ref), _f32(out)
+    bi, bj = _I(-1), _I(-1)
+    ok = lib().or_check_result(host_layout, dev_layout, nrows, ncols, _p(r), _p(o), eps,
+                               int(first_only), ctypes.byref(bi), ctypes.byref(bj))
+    return bool(ok), (bi.value, bj.value)
+
+
+def calc_max_nv(nr: int, nc: int, nnz: int, mem_bytes: int, dtype_size: int = 4,
+                maxnv: int = 128) -> int:
+    """calcMaxNv (spmvspmm_benchmark.cu:78-90)."""
+    return lib().or_calc_max_nv(nr, nc, nnz, mem_bytes, dtype_size, maxnv)
+
+
+def num_chunks(nnz: int, chunk: int) -> int:
+    return lib().or_num_chunks(nnz, chunk)
+
+
+def balanced_partition(nr: int, rowPtr, chunk: int, snap: int) -> np.ndarray:
+    rp = _i32(rowPtr)
+    n = num_chunks(int(rp[-1]), chunk)
+    meta = np.zeros(2 * (n + 1), np.int32)
+    lib().or_balanced_partition(nr, int(rp[-1]), _p(rp), chunk, snap, _p(meta))
+    return meta
+
+
+def balanced_ownership(nr: int, rowPtr, chunk: int, snap: int) -> np.ndarray:
+    rp = _i32(rowPtr)
+    own = np.zeros(2 * max(1, nr), np.int32)
+    if lib().or_balanced_ownership(nr, int(rp[-1]), _p(rp), chunk, snap, _p(own)) != 0:
+        raise AssertionError("balanced ownership walk inconsistent")
+    return own[: 2 * nr]
+
+
+def coo_ownership(nr: int, rowIdx, chunk: int) -> np.ndarray:
+    ri = _i32(rowIdx)
+    own = np.zeros(2 * max(1, nr), np.int32)
+    if lib().or_coo_ownership(nr, ri.size, _p(ri), chunk, _p(own)) != 0:
+        raise AssertionError("COO ownership walk inconsistent")
+    return own[: 2 * nr]
+
+
+_QDT = {0: np.float32, 1: np.uint16, 2: np.uint16, 3: np.uint8}
+
+
+def quantize(fmt: int, x) -> np.ndarray:
+    """Round float32 values to BF16 / FP16 / FP8-E4M3 storage (nearest even)."""
+    xf = _f32(x).reshape(-1)
+    q = np.zeros(xf.size, _QDT[fmt])
+    lib().or_quantize(fmt, xf.size, _p(xf), _p(q))
+    return q
+
+
+def dequantize(fmt: int, q) -> np.ndarray:
+    q = np.ascontiguousarray(q, _QDT[fmt]).reshape(-1)
+    x = np.zeros(q.size, np.float64)
+    lib().or_dequantize(fmt, q.size, _p(q), _p(x))
+    return x
+
+
+# ---------------------------------------------------------------- tolerances
+# FP32 parity rule, stated once for every test:
+#   (1) the reference's own check: |gpu - host_fp32| <= 1e-3 absolute
+#       (checkResult, spmvspmm_benchmark.cu:94,103);
+#   (2) against FP64: |gpu - c64| <= REL_TOL_F32 * sum_p |a_p||b_p| + 1e-30,
+#       i.e. relative to the condition scale of each element.  A recursive
+#       FP32 sum of n products has error <= n*u*sum|a||b| (u = 2^-24); the
+#       kernels' sums are shorter chains (per lane, then a tree), and for the
+#       rows here (<= 4096 nonzeros) 2e-5 covers the serial host loop too.
+REF_ABS_TOL = 1e-3
+REL_TOL_F32 = 2e-5
+
+
+def rel_err(c, c64, absc) -> float:
+    """max |c - c64| / sum|a||b| over all elements (0 where the scale is 0)."""
+    c = np.asarray(c, np.float64).reshape(-1)
+    d = np.abs(c - c64)
+    scale = np.where(absc > 0, absc, 1.0)
+    bad = (absc == 0) & (d > 0)
+    if bad.any():
+        return float("inf")
+    return float((d / scale).max()) if d.size else 0.0
