@@ -259,16 +259,9 @@ def run_ours(args):
             step()
         torch.cuda.synchronize(dev)
 
-    # main-kernel event ring for the timed region
+    # main-kernel events (library-owned, recorded on the launching stream)
     K = args.steps
-    ev_s = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
-    ev_e = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
-    arr_s = (ctypes.c_void_p * K)(*[e.cuda_event for e in ev_s])
-    arr_e = (ctypes.c_void_p * K)(*[e.cuda_event for e in ev_e])
-    for e in ev_s + ev_e:   # materialise the events on this device
-        e.record(stream)
-    torch.cuda.synchronize(dev)
-    L.daspmm_set_kernel_timer(arr_s, arr_e, K)
+    D.check(L.daspmm_kernel_timer_begin(K), "kernel_timer_begin")
 
     if pg:
         pg.barrier()
@@ -286,11 +279,14 @@ def run_ours(args):
     if pg:
         pg.barrier()
     launches = L.daspmm_launch_count() - launches0
-    L.daspmm_set_kernel_timer(None, None, 0)
+    kt = (ctypes.c_float * K)()
+    timed = L.daspmm_kernel_timer_end(kt, K)
+    if timed != K:
+        raise RuntimeError(f"kernel timer recorded {timed} of {K} calls")
     sampler.stop()
 
     ms_total = start.elapsed_time(stop)
-    kern_ms = sum(s.elapsed_time(e) for s, e in zip(ev_s, ev_e)) / K
+    kern_ms = sum(kt) / K
     nnz_total = A.nnz
     if pg:
         t = torch.tensor([ms_total, kern_ms], dtype=torch.float64, device=dev)

@@ -25,27 +25,33 @@ namespace daspmm {
 thread_local int g_last_cuda = 0;
 
 static std::atomic<long long> g_launches{0};
+// Kernel timer: library-owned event pairs, one per timed call.
 static std::mutex g_timer_mu;
 static std::vector<cudaEvent_t> g_t_start, g_t_stop;
-static int g_t_next = 0, g_t_cur = -1;
+static int g_t_next = 0;
+static thread_local int t_cur = -1;
 
 void count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 void timer_before(cudaStream_t st)
 {
+    t_cur = -1;
     std::lock_guard<std::mutex> lk(g_timer_mu);
-    g_t_cur = -1;
-    if (g_t_start.empty()) return;
-    g_t_cur = g_t_next;
-    g_t_next = (g_t_next + 1) % (int)g_t_start.size();
-    cudaEventRecord(g_t_start[g_t_cur], st);
+    if (g_t_next >= (int)g_t_start.size()) return;
+    t_cur = g_t_next++;
+    if (cudaEventRecord(g_t_start[t_cur], st) != cudaSuccess) {
+        cudaGetLastError();
+        t_cur = -1;
+    }
 }
 
 void timer_after(cudaStream_t st)
 {
+    if (t_cur < 0) return;
     std::lock_guard<std::mutex> lk(g_timer_mu);
-    if (g_t_cur >= 0 && g_t_cur < (int)g_t_stop.size()) cudaEventRecord(g_t_stop[g_t_cur], st);
-    g_t_cur = -1;
+    if (t_cur < (int)g_t_stop.size() && cudaEventRecord(g_t_stop[t_cur], st) != cudaSuccess)
+        cudaGetLastError();
+    t_cur = -1;
 }
 
 daspmm_status cuda_fail(cudaError_t e)
@@ -465,17 +471,56 @@ daspmm_status daspmm_coo_to_csr(int nr, int nnz, const int *rowIdx, int *rowPtr,
 
 long long daspmm_launch_count(void) { return g_launches.load(); }
 
-void daspmm_set_kernel_timer(void **start_events, void **stop_events, int n)
+static void timer_release()
 {
-    std::lock_guard<std::mutex> lk(g_timer_mu);
+    for (cudaEvent_t e : g_t_start) cudaEventDestroy(e);
+    for (cudaEvent_t e : g_t_stop) cudaEventDestroy(e);
     g_t_start.clear();
     g_t_stop.clear();
     g_t_next = 0;
-    g_t_cur = -1;
-    for (int i = 0; i < n && start_events && stop_events; ++i) {
-        g_t_start.push_back((cudaEvent_t)start_events[i]);
-        g_t_stop.push_back((cudaEvent_t)stop_events[i]);
+}
+
+daspmm_status daspmm_kernel_timer_begin(int n)
+{
+    if (n < 0) return DASPMM_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(g_timer_mu);
+    timer_release();
+    for (int i = 0; i < n; ++i) {
+        cudaEvent_t a, b;
+        cudaError_t e = cudaEventCreate(&a);
+        if (e == cudaSuccess) {
+            e = cudaEventCreate(&b);
+            if (e != cudaSuccess) cudaEventDestroy(a);
+        }
+        if (e != cudaSuccess) {
+            timer_release();
+            return cuda_fail(e);
+        }
+        g_t_start.push_back(a);
+        g_t_stop.push_back(b);
     }
+    return DASPMM_OK;
+}
+
+int daspmm_kernel_timer_end(float *ms_out, int n)
+{
+    std::lock_guard<std::mutex> lk(g_timer_mu);
+    const int used = g_t_next;
+    int ok = 0;
+    for (int i = 0; i < used; ++i) {
+        float ms = 0.0f;
+        cudaError_t e = cudaEventSynchronize(g_t_stop[i]);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, g_t_start[i], g_t_stop[i]);
+        if (e != cudaSuccess) {
+            g_last_cuda = (int)e;
+            timer_release();
+            return -1;
+        }
+        if (ms_out && i < n) ms_out[i] = ms;
+        ++ok;
+    }
+    timer_release();
+    return ok;
 }
 
 daspmm_status daspmm_spmm_host(const daspmm_config *cfg, int layout, int nr, int nc, int nnz,

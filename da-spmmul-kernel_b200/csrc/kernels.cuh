@@ -343,8 +343,10 @@ __global__ void __launch_bounds__(256) k_eb_coo_sr(const KArgs a)
             float my_v = 0.0f;
             if (wide && ln.l < cnt) {
                 my_r = __ldg(a.rowIdx + base + ln.l);
-                my_c = __ldg(a.colIdx + base + ln.l);
-                my_v = __ldg(a.vals + base + ln.l);
+                if constexpr (!RECORD) {  // the recording walk gets no colIdx/values
+                    my_c = __ldg(a.colIdx + base + ln.l);
+                    my_v = __ldg(a.vals + base + ln.l);
+                }
             }
             for (int t = 0; t < cnt; t += U) {
                 int rr[U], cc[U];
@@ -360,8 +362,8 @@ __global__ void __launch_bounds__(256) k_eb_coo_sr(const KArgs a)
                     } else {
                         const bool ok = t + u < cnt;
                         rr[u] = ok ? __ldg(a.rowIdx + base + t + u) : 0;
-                        cc[u] = ok ? __ldg(a.colIdx + base + t + u) : 0;
-                        vv[u] = ok ? __ldg(a.vals + base + t + u) : 0.0f;
+                        cc[u] = (ok && !RECORD) ? __ldg(a.colIdx + base + t + u) : 0;
+                        vv[u] = (ok && !RECORD) ? __ldg(a.vals + base + t + u) : 0.0f;
                     }
                 }
                 if constexpr (!RECORD) {
@@ -600,7 +602,7 @@ __global__ void __launch_bounds__(256) k_bal(const KArgs a)
             const int cnt = min(batch, k1 - base);
             int my_c = 0;
             float my_v = 0.0f;
-            if (wide && ln.l < cnt) {
+            if (!RECORD && wide && ln.l < cnt) {  // the recording walk gets no colIdx/values
                 my_c = __ldg(a.colIdx + base + ln.l);
                 my_v = __ldg(a.vals + base + ln.l);
             }
@@ -615,7 +617,7 @@ __global__ void __launch_bounds__(256) k_bal(const KArgs a)
                         cc[u] = __shfl_sync(ln.mask, my_c, src, G);
                         vv[u] = __shfl_sync(ln.mask, my_v, src, G);
                     } else {
-                        const bool ok = t + u < cnt;
+                        const bool ok = t + u < cnt && !RECORD;
                         cc[u] = ok ? __ldg(a.colIdx + base + t + u) : 0;
                         vv[u] = ok ? __ldg(a.vals + base + t + u) : 0.0f;
                     }

@@ -163,12 +163,15 @@ daspmm_status daspmm_spmm_host(const daspmm_config *cfg, int layout, int nr, int
 /* Number of kernels this library has launched in this process. */
 long long daspmm_launch_count(void);
 
-/* Kernel timing hook: while n > 0, every SpMM call records start_events[i]
- * immediately before and stop_events[i] immediately after the launch of its
- * main (gather) kernel, on the call's stream, with i cycling 0..n-1 (events
- * are cudaEvent_t passed as void*).  n = 0 switches it off.  Process-wide;
- * meant for benchmarks. */
-void daspmm_set_kernel_timer(void **start_events, void **stop_events, int n);
+/* Kernel timing for benchmarks.  After daspmm_kernel_timer_begin(n), each
+ * SpMM call (of any thread, on the current device) records a pair of CUDA
+ * events, created by the library, immediately before and after the launch of
+ * its main gather kernel on the call's stream; slots 0..n-1 are used once
+ * each, later calls are not timed.  daspmm_kernel_timer_end waits for the
+ * recorded events, writes up to n elapsed times (ms) to ms_out, releases the
+ * events and returns how many calls were timed (or -1 on a CUDA error). */
+daspmm_status daspmm_kernel_timer_begin(int n);
+int daspmm_kernel_timer_end(float *ms_out, int n);
 
 const char *daspmm_status_string(daspmm_status s);
 int daspmm_last_cuda_error(void);   /* cudaError_t of the last failure on this thread */
