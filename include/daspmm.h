@@ -159,6 +159,34 @@ daspmm_status daspmm_spmm_host(const daspmm_config *cfg, int layout, int nr, int
                                const int *colIdx, const float *values, const float *B,
                                float *C, float beta, void *stream);
 
+/* ---- No device allocation ----------------------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * -- a plugin inside an application whose own allocator owns the device's
+ * memory, or a loop that must not pay the device-wide synchronisation of
+ * cudaMalloc/cudaFree.  Same product as daspmm_spmm with
+ * DASPMM_ALG_CSR_BALANCED on the same inputs and outputs (C = A*B + beta*C,
+ * row- or col-major), but the scratch it needs lives in a fixed array of
+ * DASPMM_NOALLOC_MAX_BYTES inside the library, which every GPU that loads the
+ * library keeps until the process exits.  Nothing is allocated, by this
+ * library or any other.
+ *   - Limit: daspmm_workspace_bytes() of the DASPMM_ALG_CSR_BALANCED default
+ *     configuration (daspmm_default_config) must be <= DASPMM_NOALLOC_MAX_BYTES;
+ *     that is about 8 * ceil(nnz / chunk) * nv bytes, chunk = 128 for
+ *     row-major nv >= 128 (so nnz * nv up to about 2.6e8).  Larger problems
+ *     return DASPMM_ERR_WORKSPACE before any device work.
+ *   - The first call on each device looks up the array's device address with
+ *     that device current; make that first call before any stream capture.
+ *   - All calls on a device share the one array.  Calls that overlap on the
+ *     GPU (different streams, or different host threads, without ordering
+ *     between them) race on it; order them.  The array keeps the last call's
+ *     contents; each call writes every entry it reads, so none needs
+ *     clearing. */
+#define DASPMM_NOALLOC_MAX_BYTES (16u << 20)
+daspmm_status daspmm_spmm_noalloc(int layout, int nr, int nc, int nnz, int nv,
+                                  const int *rowPtr, const int *colIdx,
+                                  const float *values, const float *B, float *C,
+                                  float beta, void *stream);
+
 /* ---- Diagnostics ------------------------------------------------------- */
 /* Number of kernels this library has launched in this process. */
 long long daspmm_launch_count(void);
