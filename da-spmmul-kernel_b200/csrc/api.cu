@@ -9,6 +9,8 @@
 // tiles on gridDim.y), and daspmm_spmm_ex takes any legal point.
 #include "daspmm.h"
 #include "kernels.cuh"
+#include "gather_tma.cuh"
+#include "gather_lean.cuh"
 #include "internal.h"
 
 #include <cuda_runtime.h>
@@ -23,6 +25,27 @@
 namespace daspmm {
 
 thread_local int g_last_cuda = 0;
+
+int device_sms()
+{
+    static std::mutex mu;
+    static std::map<int, int> cache;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 148;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(dev);
+    if (it != cache.end()) return it->second;
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) {
+        cudaGetLastError();
+        n = 148;
+    }
+    cache[dev] = n;
+    return n;
+}
 
 static std::atomic<long long> g_launches{0};
 // Kernel timer: library-owned event pairs, one per timed call.
@@ -137,6 +160,39 @@ daspmm_status resolve(const daspmm_config *cfg, int layout, int nr, int nnz, int
     }
     r.block = cfg->block ? cfg->block : 256;
     if (r.block != 128 && r.block != 256) return DASPMM_ERR_INVALID;  // __launch_bounds__(256)
+    r.pipe = 1;
+    r.W = 0;
+    if (cfg->pipe < 0 || cfg->pipe > 4) return DASPMM_ERR_INVALID;
+    if (cfg->alg == DASPMM_ALG_CSR_BALANCED && !r.cm && cfg->pipe != 1) {
+        // TMA ring: one warp per chunk, W-float tiles (16-byte accesses, one
+        // vector per lane group slot); the explicit fields, if given, must agree
+        // tile width: the widest of 128/64/32 floats dividing nv, or 4*lanes_col
+        int Wt = nv % 128 == 0 ? 128 : (nv % 64 == 0 ? 64 : 32);
+        if (cfg->lanes_col == 8 || cfg->lanes_col == 16 || cfg->lanes_col == 32)
+            Wt = 4 * cfg->lanes_col;
+        const bool ok = nv % Wt == 0 && (!B || aligned(B, 16)) && (!C || aligned(C, 16)) &&
+                        (!cfg->vec || cfg->vec == 4) && (!cfg->cf || cfg->cf == 1) &&
+                        (!cfg->lanes_col || cfg->lanes_col == Wt / 4) &&
+                        (!cfg->lanes_nnz || cfg->lanes_nnz == 1);
+        if (cfg->pipe >= 2 && !ok) return DASPMM_ERR_UNSUPPORTED;
+        if (ok) {
+            r.pipe = cfg->pipe ? cfg->pipe : 4;
+            r.W = Wt;
+            r.V = 4; r.CF = 1; r.L = r.W / 4; r.S = 1;
+            r.block = r.pipe == 4 ? 256 : 128;
+            if (!cfg->chunk) {
+                if (r.pipe == 4) {
+                    r.chunk = 128;  // measured best on the power-law benchmark matrix
+                } else {
+                    // rings: one wave of chunks over the resident warps (12 per SM)
+                    const long long slots = (long long)device_sms() * 12;
+                    r.chunk = (int)std::max<long long>(64, ((long long)nnz + slots - 1) / slots);
+                }
+                r.nchunks = (int)std::max<long long>(1, ((long long)nnz + r.chunk - 1) / r.chunk);
+                r.snap = cfg->snap ? std::min(cfg->snap, r.chunk) : r.chunk / 2;
+            }
+        }
+    }
     const int W = r.L * r.V * r.CF;
     r.tiles = (nv + W - 1) / W;
     if (r.tiles > 65535) return DASPMM_ERR_UNSUPPORTED;
@@ -147,12 +203,62 @@ daspmm_status resolve(const daspmm_config *cfg, int layout, int nr, int nnz, int
 size_t workspace_bytes(const Resolved &r, int nv)
 {
     size_t b = 0;
-    if (r.alg == DASPMM_ALG_CSR_BALANCED) b += align256(sizeof(int2) * ((size_t)r.nchunks + 1));
+    if (r.alg == DASPMM_ALG_CSR_BALANCED) {
+        b += align256(sizeof(int2) * ((size_t)r.nchunks + 1));
+        b += align256(sizeof(int) * (size_t)r.nchunks * r.tiles);  // split-row arrival counters
+    }
     if (r.alg >= DASPMM_ALG_COO_SCALAR) b += align256(sizeof(float) * 2 * (size_t)r.nchunks * nv);
     return b;
 }
 
 // ---------------------------------------------------------------- launches
+template <int W, int NS, int MODE>
+static void launch_tma_w(const Resolved &r, const KArgs &a, cudaStream_t st)
+{
+    using R = TmaRing<W, NS>;
+    static bool attr = false;  // per process: the attribute is per function
+    if (!attr) {
+        cudaFuncSetAttribute(k_bal_tma<W, NS, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             R::kCtaBytes);
+        attr = true;
+    }
+    const unsigned gx = (unsigned)std::max<long long>(
+        1, std::min<long long>(((long long)a.nchunks + R::kWarps - 1) / R::kWarps, 148LL * 64));
+    k_bal_tma<W, NS, MODE><<<dim3(gx, r.tiles), R::kWarps * 32, R::kCtaBytes, st>>>(a);
+}
+
+template <int MODE>
+static void launch_ring(const Resolved &r, const KArgs &a, cudaStream_t st)
+{
+    if (r.W == 128) launch_tma_w<128, 4, MODE>(r, a, st);
+    else if (r.W == 64) launch_tma_w<64, 4, MODE>(r, a, st);
+    else launch_tma_w<32, 4, MODE>(r, a, st);
+}
+
+template <int W>
+static void launch_lean_w(const Resolved &r, const KArgs &a, cudaStream_t st)
+{
+    // at most the CTAs that fit at once (grid-stride over chunks beyond that):
+    // no partial second wave
+    const long long resident = (long long)device_sms() * DASPMM_LEAN_MINB;
+    const unsigned gx = (unsigned)std::max<long long>(
+        1, std::min<long long>(((long long)a.nchunks + 7) / 8, resident));
+    k_bal_lean<W, DASPMM_LEAN_U><<<dim3(gx, r.tiles), 256, 0, st>>>(a);
+}
+
+static void launch_tma(const Resolved &r, const KArgs &a, cudaStream_t st)
+{
+    if (r.pipe == 4) {
+        if (r.W == 128) launch_lean_w<128>(r, a, st);
+        else if (r.W == 64) launch_lean_w<64>(r, a, st);
+        else launch_lean_w<32>(r, a, st);
+    } else if (r.pipe == 3) {
+        launch_ring<1>(r, a, st);
+    } else {
+        launch_ring<0>(r, a, st);
+    }
+}
+
 template <bool CM, int V, int CF>
 static void launch_all(const Resolved &r, KArgs &a, dim3 grid, dim3 fix_grid, int block,
                        cudaStream_t st)
@@ -171,12 +277,13 @@ static void launch_all(const Resolved &r, KArgs &a, dim3 grid, dim3 fix_grid, in
         k_eb_coo_pr<CM, V, CF><<<grid, block, 0, st>>>(a);
         break;
     case DASPMM_ALG_CSR_BALANCED:
-        k_bal<CM, V, CF, false><<<grid, block, 0, st>>>(a);
+        if (r.pipe >= 2) launch_tma(r, a, st);
+        else k_bal<CM, V, CF, false><<<grid, block, 0, st>>>(a);
         break;
     }
     timer_after(st);
     count_launches(1);
-    if (fix && r.alg >= DASPMM_ALG_COO_SCALAR) {
+    if (fix && r.alg >= DASPMM_ALG_COO_SCALAR && !(r.alg == DASPMM_ALG_CSR_BALANCED && r.pipe == 4)) {
         if (r.alg == DASPMM_ALG_CSR_BALANCED) k_fix_bal<CM, V, CF><<<fix_grid, block, 0, st>>>(a);
         else k_fix_coo<CM, V, CF><<<fix_grid, block, 0, st>>>(a);
         count_launches(1);
@@ -249,10 +356,13 @@ daspmm_status run_resolved(const Resolved &r, int layout, int nr, int nc, int nn
         a.slots = (float *)ws;
     } else if (r.alg == DASPMM_ALG_CSR_BALANCED) {
         int2 *meta = (int2 *)ws;
+        char *p = (char *)ws + align256(sizeof(int2) * ((size_t)r.nchunks + 1));
         a.meta = meta;
-        a.slots = (float *)((char *)ws + align256(sizeof(int2) * ((size_t)r.nchunks + 1)));
+        a.cnt = (int *)p;
+        a.slots = (float *)(p + align256(sizeof(int) * (size_t)r.nchunks * r.tiles));
         const unsigned pg = (unsigned)std::max(1, (nr + 255) / 256);
-        k_partition<<<pg, 256, 0, st>>>(nr, nnz, rowPtr, r.chunk, r.snap, r.nchunks, meta);
+        k_partition<<<pg, 256, 0, st>>>(nr, nnz, rowPtr, r.chunk, r.snap, r.nchunks, meta,
+                                         a.cnt, r.tiles);
         count_launches(1);
     }
     const long long units =
@@ -417,7 +527,7 @@ daspmm_status daspmm_partition(int nr, int nnz, const int *rowPtr, int chunk, in
     const int nch = daspmm_num_chunks(nnz, chunk);
     const unsigned pg = (unsigned)std::max(1, (nr + 255) / 256);
     k_partition<<<pg, 256, 0, (cudaStream_t)stream>>>(nr, nnz, rowPtr, chunk, std::min(snap, chunk),
-                                                      nch, (int2 *)meta);
+                                                      nch, (int2 *)meta, nullptr, 1);
     count_launches(1);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? DASPMM_OK : cuda_fail(e);
@@ -470,6 +580,15 @@ daspmm_status daspmm_coo_to_csr(int nr, int nnz, const int *rowIdx, int *rowPtr,
 }
 
 long long daspmm_launch_count(void) { return g_launches.load(); }
+
+daspmm_status daspmm_device_error(void)
+{
+    int v = 0, zero = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(&v, g_device_error, sizeof(int));
+    if (e == cudaSuccess && v) e = cudaMemcpyToSymbol(g_device_error, &zero, sizeof(int));
+    if (e != cudaSuccess) return cuda_fail(e);
+    return v ? DASPMM_ERR_TIMEOUT : DASPMM_OK;
+}
 
 static void timer_release()
 {

@@ -1,0 +1,143 @@
+// gather_lean.cuh -- balanced-CSR SpMM, lean register gather at high occupancy.
+//
+// Measured on B200: gathering the B rows of the 262,144-row power-law matrix
+// in its own column order runs at ~16 TB/s out of L2 when every SM keeps 64
+// warps resident with 4 independent 16-byte loads per lane in flight; the
+// bottleneck of a gather kernel is therefore warps in flight and instructions
+// per nonzero, not the memory system.  This kernel keeps both small: one warp
+// per chunk of the balanced split (k_partition), U = 4 nonzeros per step with
+// their column/value loads broadcast to all lanes (one L1 line serves the
+// warp), one W/32-float vector of the B row per lane, row ends from a
+// 32-entry lane cache, and at most 48 registers per thread (40 warps per SM;
+// measured better than 32 or 48 warps with fewer registers).
+//
+// Same chunk boundaries, walk and ownership as k_bal.  A row split across
+// chunks is finished inside this kernel: its last piece to arrive adds all
+// pieces in chunk order (piece_arrive), so no fix-up launch is needed.
+// Row-major, nv % W == 0, B and C 16-byte aligned.
+#pragma once
+
+#include "kernels.cuh"
+#include "tma.cuh"
+
+namespace daspmm {
+
+#ifndef DASPMM_LEAN_MINB
+#define DASPMM_LEAN_MINB 5  // CTAs of 256 threads per SM: 40 warps, <= 48 registers
+#endif
+#ifndef DASPMM_LEAN_U
+#define DASPMM_LEAN_U 4     // nonzeros (B rows) in flight per warp step
+#endif
+
+template <int W, int U>
+__global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_lean(const KArgs a)
+{
+    constexpr int VL = W / 32;  // floats of the B row per lane
+    const int lane = threadIdx.x & 31;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const int tb = blockIdx.y * W + lane * VL;
+    const float *Bl = a.B + tb;
+    const uint64_t pol_once = policy_evict_first();
+
+    for (long long cl = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; cl < a.nchunks;
+         cl += nwarps) {
+        const int c = (int)cl;
+        const int2 m0 = a.meta[c], m1 = a.meta[c + 1];
+        const int k0 = m0.x, k1 = m1.x, s1 = m1.y;
+        int r = m0.y;
+        bool cont = k0 > __ldg(a.rowPtr + r);
+        // row-end cache: lane l holds rowPtr[rb + 1 + l]; the next 32 are prefetched
+        int rb = r;
+        int rc = __ldg(a.rowPtr + min(rb + 1 + lane, a.nr));
+        int rn = __ldg(a.rowPtr + min(rb + 33 + lane, a.nr));
+        int re = __shfl_sync(kFull, rc, 0);
+        float acc[VL];
+#pragma unroll
+        for (int e = 0; e < VL; ++e) acc[e] = 0.0f;
+
+        const bool head_piece = cont;  // row m0.y continues from an earlier chunk
+        auto emit = [&](int row, bool ends) {
+            if (ends && !cont) {
+                float *dst = a.C + (size_t)row * a.ldc + tb;
+                if (a.beta != 0.0f) {
+                    float old[VL];
+                    ld_plain<VL>(old, dst);
+#pragma unroll
+                    for (int e = 0; e < VL; ++e) acc[e] = fmaf(a.beta, old[e], acc[e]);
+                }
+                st_hint<VL>(dst, acc, pol_once);
+            } else {  // a piece of a row split across chunks: park it in its carry slot
+                st_v<VL>(slot_ptr(a, c, cont ? 0 : 1, tb), acc);
+            }
+#pragma unroll
+            for (int e = 0; e < VL; ++e) acc[e] = 0.0f;
+            cont = false;
+        };
+        auto step = [&](int p, float v, const float (&b)[VL]) {
+            while (p >= re) {
+                emit(r, true);
+                ++r;
+                if (r - rb >= 32) {
+                    rb += 32;
+                    rc = rn;
+                    rn = __ldg(a.rowPtr + min(rb + 33 + lane, a.nr));
+                }
+                re = __shfl_sync(kFull, rc, r - rb);
+            }
+#pragma unroll
+            for (int e = 0; e < VL; ++e) acc[e] = fmaf(v, b[e], acc[e]);
+        };
+        // Windows of 32 nonzeros: lane l holds the column/value of nonzero
+        // wb + l; the next window's are loaded while this one is gathered.
+        auto load_win = [&](int wb, int &col, float &val) {
+            const bool ok = wb + lane < k1;
+            col = ok ? ld_hint_s32(a.colIdx + wb + lane, pol_once) : 0;
+            val = ok ? ld_hint_f32(a.vals + wb + lane, pol_once) : 0.0f;
+        };
+        int ccur, cnext;
+        float vcur, vnext;
+        load_win(k0, ccur, vcur);
+        for (int wb = k0; wb < k1; wb += 32) {
+            load_win(wb + 32, cnext, vnext);
+            const int cnt = min(32, k1 - wb);
+            int t = 0;
+            for (; t + U <= cnt; t += U) {  // U rows in flight
+                int cc[U];
+                float vv[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    cc[u] = __shfl_sync(kFull, ccur, t + u);
+                    vv[u] = __shfl_sync(kFull, vcur, t + u);
+                }
+                float b[U][VL];
+#pragma unroll
+                for (int u = 0; u < U; ++u) ld_nc<VL>(b[u], Bl + (size_t)cc[u] * a.ldb);
+#pragma unroll
+                for (int u = 0; u < U; ++u) step(wb + t + u, vv[u], b[u]);
+            }
+            for (; t < cnt; ++t) {
+                float b[VL];
+                ld_nc<VL>(b, Bl + (size_t)__shfl_sync(kFull, ccur, t) * a.ldb);
+                step(wb + t, __shfl_sync(kFull, vcur, t), b);
+            }
+            ccur = cnext;
+            vcur = vnext;
+        }
+        while (r < s1) {
+            emit(r, true);
+            ++r;
+        }
+        const int head_row = m0.y;
+        bool tail_piece = false;
+        if (r < a.nr && r == s1 && __ldg(a.rowPtr + r) < k1) {
+            tail_piece = !cont;  // a continuing row here is the head piece itself
+            emit(r, false);
+        }
+        // the pieces this chunk parked arrive (at most two; fence + count, and
+        // the last piece of a row adds them all)
+        if (head_piece) piece_arrive<VL>(a, head_row, tb);
+        if (tail_piece) piece_arrive<VL>(a, s1, tb);
+    }
+}
+
+}  // namespace daspmm

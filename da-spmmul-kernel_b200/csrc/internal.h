@@ -16,7 +16,12 @@ struct Resolved {
     int V, L, S, CF;
     int chunk, snap, nchunks;
     int block, tiles;
+    int pipe;  // balanced CSR: 1 register gather, 2 TMA ring
+    int W;     // TMA ring: tile width in floats (32, 64, 128)
 };
+
+// SMs of the current device (148 when no device is visible).
+int device_sms();
 
 inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
@@ -31,6 +36,7 @@ inline daspmm_config to_config(const Resolved &r)
     c.chunk = r.chunk;
     c.snap = r.snap;
     c.block = r.block;
+    c.pipe = r.pipe;
     return c;
 }
 

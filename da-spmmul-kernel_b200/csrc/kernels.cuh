@@ -49,6 +49,8 @@ struct KArgs {
     const int2 *meta;   // balanced-CSR boundaries (k', s), nchunks + 1 entries
     float *slots;       // carries: [nchunks][2][nv] (0 = head piece, 1 = tail)
     int *own;           // ownership recording (tests): [nr][2]
+    int *cnt;           // pieces arrived per split row and column tile, at the
+                        // row's first chunk: [nchunks][tiles]
 };
 
 // ---------------------------------------------------------------- vectors
@@ -540,7 +542,7 @@ __global__ void __launch_bounds__(256) k_fix_coo(const KArgs a)
 // threshold that straddle chunk boundaries.
 // ======================================================================
 __global__ void k_partition(int nr, int nnz, const int *__restrict__ rowPtr,
-                            int chunk, int snap, int nchunks, int2 *meta)
+                            int chunk, int snap, int nchunks, int2 *meta, int *cnt, int tiles)
 {
     const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (r == 0) {
@@ -552,11 +554,65 @@ __global__ void k_partition(int nr, int nnz, const int *__restrict__ rowPtr,
     if (rs == re) return;
     long long c = ((long long)rs + chunk - 1) / chunk;
     if (c < 1) c = 1;
+    bool split = false;
     for (; c < nchunks && c * chunk < re; ++c) {
         const int k = (int)(c * chunk);
         const int kk = (k > rs && re - rs < snap) ? rs : k;
         meta[c] = make_int2(kk, (int)r);
+        split |= kk > rs;
     }
+    // a row split across chunks: its arrival counters (one per column tile)
+    // live at its first chunk
+    if (split && cnt)
+        for (int t = 0; t < tiles; ++t) cnt[(size_t)(rs / chunk) * tiles + t] = 0;
+}
+
+// Chunks holding pieces of a split row r (rows >= snap long are cut only at
+// nominal boundaries c*chunk, so the chunk of nonzero p inside r is p/chunk).
+__device__ __forceinline__ int first_chunk(int rs, int chunk) { return rs / chunk; }
+__device__ __forceinline__ int last_chunk(int re, int chunk) { return (re - 1) / chunk; }
+
+// A piece of split row `row`, already stored in its carry slot by this warp
+// (tail slot in the row's first chunk, head slot in later chunks), arrives:
+// it is counted at the row's first chunk and, if it is the last piece to
+// arrive, the warp adds all pieces in chunk order (the first chunk's tail,
+// then the heads) and stores the row: C = sum + beta*C.  VL floats per lane
+// at column `col`; all lanes of the warp call it.
+template <int VL>
+__device__ __forceinline__ void piece_arrive(const KArgs &a, int row, int col)
+{
+    const int rs = __ldg(a.rowPtr + row), re = __ldg(a.rowPtr + row + 1);
+    const int c0 = first_chunk(rs, a.chunk), c1 = last_chunk(re, a.chunk);
+    __threadfence();
+    __syncwarp();
+    int last = 0;
+    if ((threadIdx.x & 31) == 0)  // one counter per (row, column tile)
+        last = atomicAdd(a.cnt + (size_t)c0 * gridDim.y + blockIdx.y, 1) == c1 - c0;
+    last = __shfl_sync(kFull, last, 0);
+    if (!last) return;
+    __threadfence();
+    float tot[VL];
+    ld_cg<VL>(tot, slot_ptr(a, c0, 1, col));
+    constexpr int P = 4;  // independent carry loads in flight
+    for (int cb = c0 + 1; cb <= c1; cb += P) {
+        float h[P][VL];
+#pragma unroll
+        for (int u = 0; u < P; ++u)
+            if (cb + u <= c1) ld_cg<VL>(h[u], slot_ptr(a, cb + u, 0, col));
+#pragma unroll
+        for (int u = 0; u < P; ++u)
+            if (cb + u <= c1)
+#pragma unroll
+                for (int e = 0; e < VL; ++e) tot[e] += h[u][e];
+    }
+    float *dst = a.C + (size_t)row * a.ldc + col;
+    if (a.beta != 0.0f) {
+        float old[VL];
+        ld_plain<VL>(old, dst);
+#pragma unroll
+        for (int e = 0; e < VL; ++e) tot[e] = fmaf(a.beta, old[e], tot[e]);
+    }
+    st_v<VL>(dst, tot);
 }
 
 template <bool CM, int V, int CF, bool RECORD>

@@ -62,7 +62,7 @@ class Config(ctypes.Structure):
     """daspmm_config: one point of the design space (0 = library default)."""
 
     _fields_ = [(n, ctypes.c_int) for n in
-                ("alg", "vec", "lanes_col", "lanes_nnz", "cf", "chunk", "snap", "block")]
+                ("alg", "vec", "lanes_col", "lanes_nnz", "cf", "chunk", "snap", "block", "pipe")]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}

@@ -73,6 +73,11 @@ typedef struct daspmm_config {
     int chunk;      /* nonzeros per chunk for the nonzero-balanced splits */
     int snap;       /* balanced CSR: rows shorter than this are never split */
     int block;      /* threads per CTA: 128 or 256 */
+    int pipe;       /* balanced CSR, row-major: 1 = register gather; a shared-memory
+                       ring fed by 2 = TMA bulk copies, 3 = 16-byte cp.async;
+                       4 = lean register gather at high occupancy (2..4 need
+                       nv % 32 == 0 and 16-byte aligned B and C);
+                       0 = the library's choice */
 } daspmm_config;
 
 /* ---- FP32 SpMM ---------------------------------------------------------
@@ -170,10 +175,12 @@ daspmm_status daspmm_spmm_host(const daspmm_config *cfg, int layout, int nr, int
  * library keeps until the process exits.  Nothing is allocated, by this
  * library or any other.
  *   - Limit: daspmm_workspace_bytes() of the DASPMM_ALG_CSR_BALANCED default
- *     configuration (daspmm_default_config) must be <= DASPMM_NOALLOC_MAX_BYTES;
- *     that is about 8 * ceil(nnz / chunk) * nv bytes, chunk = 128 for
- *     row-major nv >= 128 (so nnz * nv up to about 2.6e8).  Larger problems
- *     return DASPMM_ERR_WORKSPACE before any device work.
+ *     configuration (daspmm_default_config) must be <= DASPMM_NOALLOC_MAX_BYTES.
+ *     That is about 8 * nchunks * nv bytes: for row-major nv a multiple of 32
+ *     the default makes one chunk per resident warp (12 per SM, 1776 on a
+ *     148-SM B200), so nv up to about 1100 fits whatever nnz is; otherwise
+ *     nchunks = ceil(nnz / 32..128).  Larger problems return
+ *     DASPMM_ERR_WORKSPACE before any device work.
  *   - The first call on each device looks up the array's device address with
  *     that device current; make that first call before any stream capture.
  *   - All calls on a device share the one array.  Calls that overlap on the
@@ -188,6 +195,11 @@ daspmm_status daspmm_spmm_noalloc(int layout, int nr, int nc, int nnz, int nv,
                                   float beta, void *stream);
 
 /* ---- Diagnostics ------------------------------------------------------- */
+/* Reads and clears the device-side error word of the current device: 0, or
+ * DASPMM_ERR_TIMEOUT if a kernel's bounded wait expired since the last call
+ * (that kernel stopped early and its output is incomplete). */
+daspmm_status daspmm_device_error(void);
+
 /* Number of kernels this library has launched in this process. */
 long long daspmm_launch_count(void);
 

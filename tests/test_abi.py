@@ -18,6 +18,8 @@ def declared_symbols():
     names = set()
     for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
         txt = open(h).read()
+        if 'extern "C"' not in txt:   # C++ drop-in headers: templates and inlines only
+            continue
         # C declarations of the ABI: "<type> daspmm_xxx(" at line start
         for m in re.finditer(r"^[A-Za-z_][\w \*]*?\b(daspmm_\w+)\s*\(", txt, re.M):
             names.add(m.group(1))
@@ -42,8 +44,16 @@ def test_abi_version_and_status_strings():
 
 def test_default_configs():
     c = D.default_config(D.Alg.CSR_BALANCED, D.Layout.ROW_MAJOR, 262144, 262144, 1_227_000, 128)
-    assert (c.vec, c.lanes_col, c.lanes_nnz, c.cf) == (4, 32, 1, 1)
-    assert c.chunk == 128 and c.snap == 64
+    assert (c.vec, c.lanes_col, c.lanes_nnz, c.cf, c.pipe) == (4, 32, 1, 1, 4)
+    assert c.chunk == 128 and c.snap == 64 and c.block == 256
+    # the TMA ring sizes one wave of chunks over 148 SMs x 12 warps (no GPU here: 148)
+    r = D.Config(alg=4, pipe=2)
+    c = D.default_config(D.Alg.CSR_BALANCED, D.Layout.ROW_MAJOR, 262144, 262144, 1_227_000, 128)
+    assert D.workspace_bytes(r, 0, 262144, 1_227_000, 128) > 0
+    c = D.default_config(D.Alg.CSR_BALANCED, D.Layout.ROW_MAJOR, 1000, 1000, 9000, 30)
+    assert c.pipe == 1 and c.chunk == 64           # nv % 32 != 0: register gather (V=2, L=16)
+    c = D.default_config(D.Alg.CSR_BALANCED, D.Layout.COL_MAJOR, 1000, 1000, 9000, 64)
+    assert c.pipe == 1
     c = D.default_config(D.Alg.CSR_VECTOR, D.Layout.ROW_MAJOR, 100, 100, 1000, 1)
     assert (c.vec, c.lanes_col, c.lanes_nnz) == (1, 1, 32)
     c = D.default_config(D.Alg.CSR_SCALAR, D.Layout.ROW_MAJOR, 100, 100, 1000, 512)

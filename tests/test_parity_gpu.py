@@ -175,12 +175,41 @@ def test_design_space_points(mats):
             _check(A, 1, nv, B, C, what=f"CM {alg.name} cf={cf}")
 
 
+@pytest.mark.parametrize("name", ["powerlaw", "hub", "uniform", "random"])
+def test_balanced_tma_ring(mats, name):
+    """The TMA-fed ring (pipe 2) against the oracle: tile widths 32/64/128,
+    several column tiles, chunk sizes that split hub rows across many chunks,
+    beta, and no expired device waits."""
+    A, dA = mats[name]
+    rng = np.random.default_rng(12)
+    for pipe in (2, 3, 4):   # TMA ring / cp.async ring / lean register gather
+        for nv in (32, 64, 96, 128, 160, 256):
+            B = rng.uniform(-1, 1, A.nc * nv).astype(np.float32)
+            for kw in ({}, dict(chunk=40, snap=9), dict(chunk=7, snap=3), dict(chunk=5000),
+                       dict(lanes_col=8, chunk=50)):   # 32-float tiles
+                cfg = D.Config(alg=int(D.Alg.CSR_BALANCED), pipe=pipe, **kw)
+                C = _run(A, dA, D.Alg.CSR_BALANCED, 0, nv, B, cfg=cfg)
+                _check(A, 0, nv, B, C, what=f"ring{pipe} {name} nv={nv} {kw}")
+        nv = 64
+        B = rng.uniform(-1, 1, A.nc * nv).astype(np.float32)
+        C0 = rng.uniform(-1, 1, A.nr * nv).astype(np.float32)
+        cfg = D.Config(alg=int(D.Alg.CSR_BALANCED), pipe=pipe, chunk=33, snap=5)
+        C = _run(A, dA, D.Alg.CSR_BALANCED, 0, nv, B, beta=0.75, C0=C0, cfg=cfg)
+        _check(A, 0, nv, B, C, beta=0.75, C0=C0, what=f"ring{pipe} beta")
+    assert D.lib().daspmm_device_error() == 0
+
+
 def test_deterministic_repeat(mats):
     A, dA = mats["hub"]
     B = np.random.default_rng(8).uniform(-1, 1, A.nc * 32).astype(np.float32)
     for alg in ALGS:
         c1 = _run(A, dA, alg, 0, 32, B)
         c2 = _run(A, dA, alg, 0, 32, B)
+        np.testing.assert_array_equal(c1, c2)
+    for pipe in (1, 2):
+        cfg = lambda: D.Config(alg=int(D.Alg.CSR_BALANCED), pipe=pipe, chunk=64)
+        c1 = _run(A, dA, D.Alg.CSR_BALANCED, 0, 32, B, cfg=cfg())
+        c2 = _run(A, dA, D.Alg.CSR_BALANCED, 0, 32, B, cfg=cfg())
         np.testing.assert_array_equal(c1, c2)
 
 

@@ -93,10 +93,10 @@ def test_full_size_power_law_fits_and_matches(cuda):
 
 def test_too_large_is_refused_before_device_work(cuda):
     import torch
-    # 2.2M nonzeros x 128 columns needs ~17.6 MB of carries: over the 16 MiB limit
+    # one chunk per resident warp x 4096 columns x 8 bytes: far over the 16 MiB limit
     nr = 1 << 20
     nnz = 2_200_000
-    nv = 128
+    nv = 4096
     cfg = D.default_config(D.Alg.CSR_BALANCED, 0, nr, nr, nnz, nv)
     assert D.workspace_bytes(cfg, 0, nr, nnz, nv) > (16 << 20)
     dummy = torch.zeros(4, dtype=torch.float32, device="cuda")
