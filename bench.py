@@ -320,6 +320,7 @@ def run_ours(args):
         e2e = None
         if not args.no_e2e:
             e2e = run_e2e(D, A, B, dev, alg, min(K, args.e2e_steps))
+        mixed = None if args.no_mixed else run_mixed(D, A, dA, B, dev, K, peak)
         clk = sampler.summary()
         clk_in = sampler.summary(t0, t1)
         clocks = {"sm_mhz": clk_in["sm_mhz"] if clk_in["samples"] else clk["sm_mhz"],
@@ -345,6 +346,7 @@ def run_ours(args):
                          "peak_source": peak_src},
             "step_hbm_gbs": round(abytes / (ms_step * 1e-3) / 1e9, 1),
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": int(launches),
+            "mixed": mixed,
         }
     if pg:
         pg.barrier()
@@ -352,6 +354,46 @@ def run_ours(args):
     if line is not None:
         print(json.dumps(line), flush=True)
     return 0
+
+
+def run_mixed(D, A, dA, B, dev, steps, peak):
+    """Same SpMM with BF16 storage (values and B) and with BF16 values + FP8
+    E4M3 B (per-column scales): FP32 accumulation, kernel-timed.  Errors of
+    these forms against the FP64 oracle are stated by tests/test_mixed_gpu.py
+    (BF16 <= 1e-2, E4M3 <= 2^-4 max-norm relative)."""
+    import torch
+    L = D.lib()
+    Bt = torch.from_numpy(B).to(dev)
+    vt = torch.from_numpy(A.values).to(dev)
+    out = {}
+    C = torch.zeros(A.nr * NV, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    for name, vf, bf in (("bf16", D.Fmt.BF16, D.Fmt.BF16), ("bf16_e4m3", D.Fmt.BF16, D.Fmt.E4M3)):
+        vq = D.quantize(vt, vf)
+        scales = D.e4m3_scales(Bt, A.nc, NV) if bf == D.Fmt.E4M3 else None
+        bq = D.quantize(Bt, bf, scales, NV if scales is not None else 0)
+        run = lambda: D.spmm_mixed(dA, vq, vf, bq, bf, C, NV, b_scales=scales, stream=stream)
+        for _ in range(5):
+            run()
+        torch.cuda.synchronize(dev)
+        D.check(L.daspmm_kernel_timer_begin(steps), "kernel_timer_begin")
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for _ in range(steps):
+            run()
+        e.record(stream)
+        torch.cuda.synchronize(dev)
+        kt = (ctypes.c_float * steps)()
+        n = L.daspmm_kernel_timer_end(kt, steps)
+        ms = s.elapsed_time(e) / steps
+        kms = sum(kt) / max(1, n)
+        sb = 2 if bf == D.Fmt.BF16 else 1
+        abytes = algorithmic_bytes(A, NV, s_val=2, s_b=sb) + (4 * NV if sb == 1 else 0)
+        out[name] = {"value": round(2.0 * A.nnz * NV / (ms * 1e-3) / 1e9, 3), "unit": UNIT,
+                     "ms_per_step": round(ms, 5), "kernel_ms": round(kms, 5),
+                     "algorithmic_bytes": abytes,
+                     "roofline_frac": round(abytes / (kms * 1e-3) / 1e9 / peak, 4)}
+    return out
 
 
 def run_e2e(D, A, B, dev, alg, steps):
@@ -399,6 +441,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -15,12 +15,80 @@
 // chunks is finished inside this kernel: its last piece to arrive adds all
 // pieces in chunk order (piece_arrive), so no fix-up launch is needed.
 // Row-major, nv % W == 0, B and C 16-byte aligned.
+//
+// Storage types (mixed precision): values TV in {float, bf16, fp16}, B in
+// TB in {float, bf16, fp16, fp8 e4m3}; products and sums are FP32.  For FP8
+// B, column k carries an FP32 scale (B = q * scale[k]); sums are taken over
+// the unscaled q and each output column is scaled once, when its row is
+// stored.  With KAHAN, rows of at least kahan_min nonzeros are summed with
+// Kahan compensation (each piece of a split row included).
 #pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_fp8.h>
 
 #include "kernels.cuh"
 #include "tma.cuh"
 
 namespace daspmm {
+
+using bf16 = __nv_bfloat16;
+using fp16 = __half;
+using fp8 = __nv_fp8_e4m3;
+
+// N consecutive elements of B (storage type T) as floats, one vector load.
+template <typename T, int N>
+__device__ __forceinline__ void ld_b(float (&r)[N], const T *p)
+{
+    if constexpr (std::is_same<T, float>::value) {
+        ld_nc<N>(r, reinterpret_cast<const float *>(p));
+    } else if constexpr (sizeof(T) == 2) {
+        // 2-byte types: N = 4 -> 8 bytes, 2 -> 4 bytes, 1 -> 2 bytes
+        uint32_t w[(N + 1) / 2];
+        if constexpr (N == 4) {
+            const uint2 t = __ldg(reinterpret_cast<const uint2 *>(p));
+            w[0] = t.x; w[1] = t.y;
+        } else if constexpr (N == 2) {
+            w[0] = __ldg(reinterpret_cast<const unsigned int *>(p));
+        } else {
+            w[0] = __ldg(reinterpret_cast<const unsigned short *>(p));
+        }
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            const unsigned short h = (unsigned short)(w[i / 2] >> (16 * (i & 1)));
+            if constexpr (std::is_same<T, bf16>::value) r[i] = __uint_as_float((uint32_t)h << 16);
+            else r[i] = __half2float(__ushort_as_half(h));
+        }
+    } else {  // fp8 e4m3: N bytes
+        uint32_t w;
+        if constexpr (N == 4) w = __ldg(reinterpret_cast<const unsigned int *>(p));
+        else if constexpr (N == 2) w = __ldg(reinterpret_cast<const unsigned short *>(p));
+        else w = __ldg(reinterpret_cast<const unsigned char *>(p));
+#pragma unroll
+        for (int i = 0; i < N; i += 2) {
+            const __half2_raw h2 =
+                __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(w >> (8 * i)), __NV_E4M3);
+            const float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&h2));
+            r[i] = f.x;
+            if (i + 1 < N) r[i + 1] = f.y;
+        }
+    }
+}
+
+// One value of A (storage type T) as float, L2 hint.
+template <typename T>
+__device__ __forceinline__ float ld_val(const T *p, uint64_t pol)
+{
+    if constexpr (std::is_same<T, float>::value) {
+        return ld_hint_f32(reinterpret_cast<const float *>(p), pol);
+    } else {
+        unsigned short h;
+        asm("ld.global.nc.L2::cache_hint.u16 %0, [%1], %2;" : "=h"(h) : "l"(p), "l"(pol));
+        if constexpr (std::is_same<T, bf16>::value) return __uint_as_float((uint32_t)h << 16);
+        else return __half2float(__ushort_as_half(h));
+    }
+}
 
 #ifndef DASPMM_LEAN_MINB
 #define DASPMM_LEAN_MINB 5  // CTAs of 256 threads per SM: 40 warps, <= 48 registers
@@ -29,15 +97,20 @@ namespace daspmm {
 #define DASPMM_LEAN_U 4     // nonzeros (B rows) in flight per warp step
 #endif
 
-template <int W, int U>
+template <int W, int U, typename TV = float, typename TB = float, bool KAHAN = false>
 __global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_lean(const KArgs a)
 {
-    constexpr int VL = W / 32;  // floats of the B row per lane
+    constexpr int VL = W / 32;  // elements of the B row per lane
+    constexpr bool SCALED = std::is_same<TB, fp8>::value;
     const int lane = threadIdx.x & 31;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     const int tb = blockIdx.y * W + lane * VL;
-    const float *Bl = a.B + tb;
+    const TB *Bl = reinterpret_cast<const TB *>(a.B) + tb;
+    const TV *Av = reinterpret_cast<const TV *>(a.vals);
     const uint64_t pol_once = policy_evict_first();
+    float sc[VL];
+#pragma unroll
+    for (int e = 0; e < VL; ++e) sc[e] = SCALED ? __ldg(a.bscale + tb + e) : 1.0f;
 
     for (long long cl = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; cl < a.nchunks;
          cl += nwarps) {
@@ -51,12 +124,19 @@ __global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_lean(const KArgs 
         int rc = __ldg(a.rowPtr + min(rb + 1 + lane, a.nr));
         int rn = __ldg(a.rowPtr + min(rb + 33 + lane, a.nr));
         int re = __shfl_sync(kFull, rc, 0);
-        float acc[VL];
+        float acc[VL], comp[VL];
 #pragma unroll
-        for (int e = 0; e < VL; ++e) acc[e] = 0.0f;
+        for (int e = 0; e < VL; ++e) acc[e] = comp[e] = 0.0f;
+        // Kahan rows: length of the current row (its start is the previous end)
+        int rs = KAHAN ? __ldg(a.rowPtr + r) : 0;
+        bool kh = KAHAN && re - rs >= a.kahan_min;
 
         const bool head_piece = cont;  // row m0.y continues from an earlier chunk
         auto emit = [&](int row, bool ends) {
+            if constexpr (SCALED) {
+#pragma unroll
+                for (int e = 0; e < VL; ++e) acc[e] *= sc[e];
+            }
             if (ends && !cont) {
                 float *dst = a.C + (size_t)row * a.ldc + tb;
                 if (a.beta != 0.0f) {
@@ -70,7 +150,7 @@ __global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_lean(const KArgs 
                 st_v<VL>(slot_ptr(a, c, cont ? 0 : 1, tb), acc);
             }
 #pragma unroll
-            for (int e = 0; e < VL; ++e) acc[e] = 0.0f;
+            for (int e = 0; e < VL; ++e) acc[e] = comp[e] = 0.0f;
             cont = false;
         };
         auto step = [&](int p, float v, const float (&b)[VL]) {
@@ -82,17 +162,29 @@ __global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_lean(const KArgs 
                     rc = rn;
                     rn = __ldg(a.rowPtr + min(rb + 33 + lane, a.nr));
                 }
+                if constexpr (KAHAN) rs = re;
                 re = __shfl_sync(kFull, rc, r - rb);
+                if constexpr (KAHAN) kh = re - rs >= a.kahan_min;
             }
+            if (KAHAN && kh) {
 #pragma unroll
-            for (int e = 0; e < VL; ++e) acc[e] = fmaf(v, b[e], acc[e]);
+                for (int e = 0; e < VL; ++e) {  // Kahan: carry the rounding error along
+                    const float y = fmaf(v, b[e], -comp[e]);
+                    const float t = acc[e] + y;
+                    comp[e] = (t - acc[e]) - y;
+                    acc[e] = t;
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < VL; ++e) acc[e] = fmaf(v, b[e], acc[e]);
+            }
         };
         // Windows of 32 nonzeros: lane l holds the column/value of nonzero
         // wb + l; the next window's are loaded while this one is gathered.
         auto load_win = [&](int wb, int &col, float &val) {
             const bool ok = wb + lane < k1;
             col = ok ? ld_hint_s32(a.colIdx + wb + lane, pol_once) : 0;
-            val = ok ? ld_hint_f32(a.vals + wb + lane, pol_once) : 0.0f;
+            val = ok ? ld_val<TV>(Av + wb + lane, pol_once) : 0.0f;
         };
         int ccur, cnext;
         float vcur, vnext;
@@ -111,13 +203,13 @@ __global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_lean(const KArgs 
                 }
                 float b[U][VL];
 #pragma unroll
-                for (int u = 0; u < U; ++u) ld_nc<VL>(b[u], Bl + (size_t)cc[u] * a.ldb);
+                for (int u = 0; u < U; ++u) ld_b<TB, VL>(b[u], Bl + (size_t)cc[u] * a.ldb);
 #pragma unroll
                 for (int u = 0; u < U; ++u) step(wb + t + u, vv[u], b[u]);
             }
             for (; t < cnt; ++t) {
                 float b[VL];
-                ld_nc<VL>(b, Bl + (size_t)__shfl_sync(kFull, ccur, t) * a.ldb);
+                ld_b<TB, VL>(b, Bl + (size_t)__shfl_sync(kFull, ccur, t) * a.ldb);
                 step(wb + t, __shfl_sync(kFull, vcur, t), b);
             }
             ccur = cnext;

@@ -29,6 +29,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace daspmm {
 
 constexpr unsigned kFull = 0xffffffffu;
@@ -51,6 +53,8 @@ struct KArgs {
     int *own;           // ownership recording (tests): [nr][2]
     int *cnt;           // pieces arrived per split row and column tile, at the
                         // row's first chunk: [nchunks][tiles]
+    const float *bscale;  // FP8 B: per-column scales
+    int kahan_min;        // rows at least this long use compensated sums
 };
 
 // ---------------------------------------------------------------- vectors
@@ -541,7 +545,7 @@ __global__ void __launch_bounds__(256) k_fix_coo(const KArgs a)
 // in lanes; k_fix_bal adds the carries of rows longer than the snap
 // threshold that straddle chunk boundaries.
 // ======================================================================
-__global__ void k_partition(int nr, int nnz, const int *__restrict__ rowPtr,
+static __global__ void k_partition(int nr, int nnz, const int *__restrict__ rowPtr,
                             int chunk, int snap, int nchunks, int2 *meta, int *cnt, int tiles)
 {
     const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -758,7 +762,7 @@ __global__ void __launch_bounds__(256) k_fix_bal(const KArgs a)
 
 // C = beta * C over an nr x nv block (used before COO accumulation when
 // beta != 1, since COO never visits rows without nonzeros).
-__global__ void k_scale(float *C, size_t n, float beta)
+static __global__ void k_scale(float *C, size_t n, float beta)
 {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (size_t)gridDim.x * blockDim.x)
@@ -769,7 +773,7 @@ __global__ void k_scale(float *C, size_t n, float beta)
 // nonzero p whose row differs from its predecessor's fills the pointers of
 // the rows in between (empty rows included).  Bit-exact with
 // generateCsrRowPtrArray (spmvspmm_benchmark.cu:41-76).
-__global__ void k_coo_to_csr(int nr, int nnz, const int *__restrict__ rowIdx, int *rowPtr)
+static __global__ void k_coo_to_csr(int nr, int nnz, const int *__restrict__ rowIdx, int *rowPtr)
 {
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p > nnz) return;
@@ -780,12 +784,12 @@ __global__ void k_coo_to_csr(int nr, int nnz, const int *__restrict__ rowIdx, in
 
 // Ownership recording buffers (tests): owner = INT_MAX / pieces = 0, then
 // unowned rows back to -1 after the walk.
-__global__ void k_own_init(int *own, int nr)
+static __global__ void k_own_init(int *own, int nr)
 {
     const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (r < nr) { own[2 * r] = 0x7fffffff; own[2 * r + 1] = 0; }
 }
-__global__ void k_own_fini(int *own, int nr)
+static __global__ void k_own_fini(int *own, int nr)
 {
     const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (r < nr && own[2 * r] == 0x7fffffff) own[2 * r] = -1;

@@ -305,6 +305,41 @@ def coo_to_csr(nr: int, rowIdx, stream=None):
     return rp
 
 
+# ---------------------------------------------------------------- mixed precision
+_TORCH_STORE = {Fmt.BF16: "bfloat16", Fmt.F16: "float16", Fmt.E4M3: "uint8"}
+
+
+def quantize(x, fmt: int, col_scales=None, ncols: int = 0, stream=None):
+    """Device round-to-nearest-even of an FP32 tensor to BF16 / FP16 / E4M3
+    (E4M3 returned as uint8 codes), optionally dividing by per-column scales."""
+    import torch
+    fmt = Fmt(fmt)
+    q = torch.empty(x.numel(), dtype=getattr(torch, _TORCH_STORE[fmt]), device=x.device)
+    check(_lib().daspmm_quantize(int(fmt), x.numel(), _dptr(x), _dptr(q), _dptr(col_scales),
+                                 ncols, _stream_ptr(stream)), "quantize")
+    return q
+
+
+def e4m3_scales(B, nrows: int, ncols: int, stream=None):
+    """Per-column FP32 scales max|B[:,k]|/448 of a row-major FP32 matrix."""
+    import torch
+    s = torch.empty(ncols, dtype=torch.float32, device=B.device)
+    check(_lib().daspmm_e4m3_scales(nrows, ncols, _dptr(B), _dptr(s), _stream_ptr(stream)),
+          "e4m3_scales")
+    return s
+
+
+def spmm_mixed(A: DeviceCsr, values, val_fmt: int, B, b_fmt: int, C, nv: int,
+               b_scales=None, beta: float = 0.0, kahan_min: int = 0, cfg: Config | None = None,
+               stream=None) -> None:
+    """C (FP32) = A*B + beta*C with values / B in reduced-precision storage."""
+    check(_lib().daspmm_spmm_mixed(ctypes.byref(cfg) if cfg is not None else None, 0, A.nr,
+                                   A.nc, A.nnz, nv, _dptr(A.rowPtr), _dptr(A.colIdx),
+                                   _dptr(values), int(val_fmt), _dptr(B), int(b_fmt),
+                                   _dptr(b_scales), _dptr(C), float(beta), int(kahan_min), None,
+                                   0, _stream_ptr(stream)), "spmm_mixed")
+
+
 # ---------------------------------------------------------------- problem
 class SpmvSpmmProblem:
     """Non-owning view of device buffers with run/benchmark, after

@@ -14,6 +14,11 @@ def apply(lib, Config):
         "daspmm_spmm_host": (_I, [ctypes.POINTER(Config), _I, _I, _I, _I, _I, _VP, _VP, _VP,
                                   _VP, _VP, _VP, ctypes.c_float, _VP]),
         "daspmm_launch_count": (ctypes.c_longlong, []),
+        "daspmm_spmm_mixed": (_I, [ctypes.POINTER(Config), _I, _I, _I, _I, _I, _VP, _VP, _VP, _I,
+                                   _VP, _I, _VP, _VP, ctypes.c_float, _I, _VP, ctypes.c_size_t,
+                                   _VP]),
+        "daspmm_quantize": (_I, [_I, ctypes.c_size_t, _VP, _VP, _VP, _I, _VP]),
+        "daspmm_e4m3_scales": (_I, [_I, _I, _VP, _VP, _VP]),
         "daspmm_device_error": (_I, []),
         "daspmm_kernel_timer_begin": (_I, [_I]),
         "daspmm_kernel_timer_end": (_I, [ctypes.POINTER(ctypes.c_float), _I]),

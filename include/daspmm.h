@@ -151,6 +151,33 @@ daspmm_status daspmm_ownership(int alg, int nr, int nnz, const int *rowPtr,
 daspmm_status daspmm_coo_to_csr(int nr, int nnz, const int *rowIdx, int *rowPtr,
                                 void *stream);
 
+/* ---- Mixed precision ---------------------------------------------------
+ * C (FP32, row-major) = A*B + beta*C with A's values stored as val_fmt and B
+ * as b_fmt; products and sums in FP32.  Supported (val_fmt, b_fmt):
+ * (F32,F32), (BF16,BF16), (F16,F16), (F32,E4M3), (BF16,E4M3).  For E4M3, B
+ * holds q with B[i,k] ~ q[i,k] * b_scales[k] (FP32 per-column scales, e.g.
+ * from daspmm_e4m3_scales).  kahan_min > 0: rows with at least that many
+ * nonzeros are summed with Kahan compensation.  Balanced-CSR split, row-major,
+ * nv a multiple of 32; B aligned to its vector access (8 bytes for 16-bit,
+ * 4 for FP8 at nv % 128 == 0).  workspace NULL: the library's per-stream one.
+ * Extends the reference's FP32-only kernels (spmm.h:17-18: values and B are
+ * float). */
+daspmm_status daspmm_spmm_mixed(const daspmm_config *cfg, int layout, int nr, int nc,
+                                int nnz, int nv, const int *rowPtr, const int *colIdx,
+                                const void *values, int val_fmt, const void *B, int b_fmt,
+                                const float *b_scales, float *C, float beta, int kahan_min,
+                                void *workspace, size_t ws_bytes, void *stream);
+
+/* q[i] = round_to_nearest_even(x[i] / col_scales[i % ncols]) in fmt (BF16,
+ * F16, or E4M3 saturating to +-448); col_scales may be NULL (no division). */
+daspmm_status daspmm_quantize(int fmt, size_t n, const float *x, void *q,
+                              const float *col_scales, int ncols, void *stream);
+
+/* Per-column E4M3 scales of a row-major nrows x ncols FP32 matrix:
+ * scales[k] = max_i |B[i,k]| / 448 (1 for an all-zero column). */
+daspmm_status daspmm_e4m3_scales(int nrows, int ncols, const float *B, float *scales,
+                                 void *stream);
+
 /* ---- Host buffers ------------------------------------------------------
  * The same product with A, B and C in HOST memory (pinned or pageable): the
  * library copies A and B to device buffers it keeps per (device, stream),

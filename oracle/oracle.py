@@ -209,6 +209,24 @@ REF_ABS_TOL = 1e-3
 REL_TOL_F32 = 2e-5
 
 
+# Mixed precision (storage in BF16 / FP16 / E4M3, FP32 arithmetic): the error
+# statement is max |c - c64| / max sum_p |a_p||b_p| over the whole result (a
+# max-norm relative error).  A per-element bound cannot hold for reduced
+# storage: a one-term output whose operand rounds to a subnormal or to zero is
+# off by up to 100% of itself.  Bounds: BF16 / FP16 storage <= 1e-2 (rounding
+# 2^-9 / 2^-12 per operand); E4M3 B <= 2^-4 (3-bit mantissa, rounding 2^-4).
+MIXED_TOL = 1e-2
+E4M3_TOL = 2.0 ** -4
+
+
+def rel_err_max(c, c64, absc) -> float:
+    """max |c - c64| / max sum|a||b| (0 for an all-zero product)."""
+    c = np.asarray(c, np.float64).reshape(-1)
+    m = float(np.max(absc)) if np.size(absc) else 0.0
+    d = float(np.max(np.abs(c - c64))) if c.size else 0.0
+    return d / m if m > 0 else (0.0 if d == 0 else float("inf"))
+
+
 def rel_err(c, c64, absc) -> float:
     """max |c - c64| / sum|a||b| over all elements (0 where the scale is 0)."""
     c = np.asarray(c, np.float64).reshape(-1)
