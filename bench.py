@@ -321,6 +321,7 @@ def run_ours(args):
         if not args.no_e2e:
             e2e = run_e2e(D, A, B, dev, alg, min(K, args.e2e_steps))
         mixed = None if args.no_mixed else run_mixed(D, A, dA, B, dev, K, peak)
+        batched = None if (args.no_batched or world > 1) else run_batched(D, dev)
         clk = sampler.summary()
         clk_in = sampler.summary(t0, t1)
         clocks = {"sm_mhz": clk_in["sm_mhz"] if clk_in["samples"] else clk["sm_mhz"],
@@ -346,7 +347,7 @@ def run_ours(args):
                          "peak_source": peak_src},
             "step_hbm_gbs": round(abytes / (ms_step * 1e-3) / 1e9, 1),
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": int(launches),
-            "mixed": mixed,
+            "mixed": mixed, "batched": batched,
         }
     if pg:
         pg.barrier()
@@ -396,6 +397,81 @@ def run_mixed(D, A, dA, B, dev, steps, peak):
     return out
 
 
+def run_batched(D, dev, reps: int = 20):
+    """The batched configuration: 512 instances (rows log-uniform in [1k, 64k],
+    average degree log-uniform in [2, 64], power-law rows), N = 64, FP32 values,
+    BF16 B, FP32 accumulation; one persistent launch per batch, row-tile size
+    autotuned, replayed from a captured CUDA graph.  Against it: the plain FP32
+    path, one daspmm_spmm launch per instance."""
+    import torch
+    import daspmm.workloads as WL
+    nv = 64
+    mats = WL.config4(512)
+    inst, plain = [], []
+    for i, A in enumerate(mats):
+        dA = D.DeviceCsr(A, dev)
+        B32 = torch.from_numpy(D.gen_dense(A.nc * nv, seed=10 + i)).to(dev)
+        C = torch.zeros(A.nr * nv, dtype=torch.float32, device=dev)
+        inst.append(dict(A=dA, nv=nv, values=dA.values, val_fmt=D.Fmt.F32,
+                         B=D.quantize(B32, D.Fmt.BF16), b_fmt=D.Fmt.BF16, C=C))
+        plain.append((dA, B32, torch.zeros_like(C)))
+    total_nnz = sum(A.nnz for A in mats)
+    chunk, _ = D.Batch.tune(inst, chunks=[128, 256, 512, 1024], reps=3)
+    batch = D.Batch(inst, chunk=chunk)
+    s = torch.cuda.Stream(dev)
+    batch.capture(s)
+    for _ in range(3):
+        batch.replay(s)
+    s.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(reps):
+        batch.replay(s)
+    e1.record(s)
+    e1.synchronize()
+    ms_b = e0.elapsed_time(e1) / reps
+    # plain FP32, one launch per instance, same stream
+    with torch.cuda.stream(s):
+        def one_pass():
+            for dA, B32, C in plain:
+                D.spmm(D.Alg.CSR_BALANCED, 0, dA, B32, C, nv=nv, stream=s)
+        one_pass()
+        s.synchronize()
+        e0.record(s)
+        for _ in range(max(1, reps // 4)):
+            one_pass()
+        e1.record(s)
+        e1.synchronize()
+    ms_p = e0.elapsed_time(e1) / max(1, reps // 4)
+    # the same 512 launches captured once into a CUDA graph (no host launch cost)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s, capture_error_mode="thread_local"):
+        one_pass()
+    with torch.cuda.stream(s):          # replay() launches on the current stream
+        for _ in range(2):
+            g.replay()
+        s.synchronize()
+        e0.record(s)
+        for _ in range(reps):
+            g.replay()
+        e1.record(s)
+        e1.synchronize()
+    ms_g = e0.elapsed_time(e1) / reps
+    del g
+    items, _ = batch.info()
+    batch.close()
+    flop = 2.0 * total_nnz * nv
+    return {"instances": len(mats), "total_nnz": total_nnz, "nv": nv, "items": items,
+            "chunk_autotuned": chunk, "storage": "FP32 values, BF16 B, FP32 accumulate",
+            "value": round(flop / (ms_b * 1e-3) / 1e9, 3), "unit": UNIT, "ms_per_batch": round(ms_b, 4),
+            "plain_fp32_one_launch_per_instance": {"value": round(flop / (ms_p * 1e-3) / 1e9, 3),
+                                                   "ms_per_batch": round(ms_p, 4)},
+            "plain_fp32_graph_replayed": {"value": round(flop / (ms_g * 1e-3) / 1e9, 3),
+                                          "ms_per_batch": round(ms_g, 4)},
+            "speedup_vs_plain": round(ms_p / ms_b, 3),
+            "speedup_vs_plain_graph": round(ms_g / ms_b, 3)}
+
+
 def run_e2e(D, A, B, dev, alg, steps):
     """Same SpMM through daspmm_spmm_host: pinned host A, B in; C out."""
     import numpy as np
@@ -442,6 +518,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

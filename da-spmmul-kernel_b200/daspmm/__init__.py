@@ -340,6 +340,98 @@ def spmm_mixed(A: DeviceCsr, values, val_fmt: int, B, b_fmt: int, C, nv: int,
                                    0, _stream_ptr(stream)), "spmm_mixed")
 
 
+# ---------------------------------------------------------------- autotuner
+def autotune(layout: int, A: DeviceCsr, B, C, nv: int, reps: int = 5, use_coo: bool = True,
+             stream=None):
+    """Times the design-space candidates on this problem and caches the best
+    for DASPMM_ALG_AUTO; returns (Config, microseconds per call)."""
+    cfg = Config()
+    us = ctypes.c_float()
+    check(_lib().daspmm_autotune(int(layout), A.nr, A.nc, A.nnz, nv, _dptr(A.rowPtr),
+                                 _dptr(A.rowIdx) if use_coo else None, _dptr(A.colIdx),
+                                 _dptr(A.values), _dptr(B), _dptr(C), reps, ctypes.byref(cfg),
+                                 ctypes.byref(us), _stream_ptr(stream)), "autotune")
+    return cfg, us.value
+
+
+def fingerprint(layout: int, A: DeviceCsr, nv: int, dtype: int = 0, stream=None) -> dict:
+    from ._sigs import Fingerprint
+    fp = Fingerprint()
+    check(_lib().daspmm_fingerprint_of(int(layout), A.nr, A.nnz, nv, dtype, _dptr(A.rowPtr),
+                                       _stream_ptr(stream), ctypes.byref(fp)), "fingerprint")
+    return {n: getattr(fp, n) for n, _ in fp._fields_}
+
+
+# ---------------------------------------------------------------- batches
+class Batch:
+    """Many SpMMs in one persistent launch (daspmm_batch_*).
+
+    `instances` is a list of dicts with keys A (DeviceCsr), values (device
+    tensor, F32 or BF16), B, C (device tensors), nv, optional val_fmt, b_fmt,
+    b_scales, beta.  The tensors must outlive the batch."""
+
+    def __init__(self, instances, chunk: int = 0, stream=None):
+        from ._sigs import Instance
+        self._keep = instances
+        arr = (Instance * max(1, len(instances)))()
+        for i, d in enumerate(instances):
+            A = d["A"]
+            arr[i] = Instance(A.nr, A.nc, A.nnz, d["nv"], _dptr(A.rowPtr) or 0,
+                              _dptr(A.colIdx) or 0, _dptr(d.get("values", A.values)) or 0,
+                              int(d.get("val_fmt", Fmt.F32)), _dptr(d["B"]) or 0,
+                              int(d.get("b_fmt", Fmt.F32)), _dptr(d.get("b_scales")) or 0,
+                              _dptr(d["C"]) or 0, float(d.get("beta", 0.0)))
+        self._h = ctypes.c_void_p()
+        cfg = Config(chunk=chunk)
+        check(_lib().daspmm_batch_create(arr, len(instances), ctypes.byref(cfg),
+                                         ctypes.byref(self._h), _stream_ptr(stream)),
+              "batch_create")
+
+    def run(self, stream=None):
+        check(_lib().daspmm_batch_run(self._h, _stream_ptr(stream)), "batch_run")
+
+    def capture(self, stream):
+        check(_lib().daspmm_batch_capture(self._h, _stream_ptr(stream)), "batch_capture")
+
+    def replay(self, stream):
+        check(_lib().daspmm_batch_replay(self._h, _stream_ptr(stream)), "batch_replay")
+
+    @staticmethod
+    def tune(instances, chunks=None, reps: int = 5, stream=None):
+        """Fastest row-tile size for this set of instances: (chunk, us)."""
+        from ._sigs import Instance
+        arr = (Instance * max(1, len(instances)))()
+        for i, d in enumerate(instances):
+            A = d["A"]
+            arr[i] = Instance(A.nr, A.nc, A.nnz, d["nv"], _dptr(A.rowPtr) or 0,
+                              _dptr(A.colIdx) or 0, _dptr(d.get("values", A.values)) or 0,
+                              int(d.get("val_fmt", Fmt.F32)), _dptr(d["B"]) or 0,
+                              int(d.get("b_fmt", Fmt.F32)), _dptr(d.get("b_scales")) or 0,
+                              _dptr(d["C"]) or 0, float(d.get("beta", 0.0)))
+        ch = (ctypes.c_int * len(chunks))(*chunks) if chunks else None
+        best, us = ctypes.c_int(), ctypes.c_float()
+        check(_lib().daspmm_batch_tune(arr, len(instances), ch, len(chunks) if chunks else 0,
+                                       reps, ctypes.byref(best), ctypes.byref(us),
+                                       _stream_ptr(stream)), "batch_tune")
+        return best.value, us.value
+
+    def info(self):
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        check(_lib().daspmm_batch_info(self._h, ctypes.byref(a), ctypes.byref(b)), "batch_info")
+        return a.value, b.value
+
+    def close(self):
+        if self._h:
+            _lib().daspmm_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # ---------------------------------------------------------------- problem
 class SpmvSpmmProblem:
     """Non-owning view of device buffers with run/benchmark, after

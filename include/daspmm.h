@@ -114,6 +114,33 @@ size_t daspmm_workspace_bytes(const daspmm_config *cfg, int layout, int nr, int 
 daspmm_status daspmm_default_config(int alg, int layout, int nr, int nc, int nnz,
                                     int nv, daspmm_config *out);
 
+/* ---- Autotuner ---------------------------------------------------------
+ * No counterpart in the reference: its caller picks alg (spmvspmm.h:57-58).
+ * A fingerprint of a problem: shape, storage and row-length quantiles
+ * (computed on the device from rowPtr; quantiles are the upper edges of
+ * power-of-two length buckets, capped at the maximum). */
+typedef struct daspmm_fingerprint {
+    int layout, nv, dtype, nr, nnz;
+    int p50, p90, p99, max_row;
+} daspmm_fingerprint;
+
+daspmm_status daspmm_fingerprint_of(int layout, int nr, int nnz, int nv, int dtype,
+                                    const int *rowPtr, void *stream, daspmm_fingerprint *out);
+
+/* Times the design-space candidates that apply (reps calls each, after two
+ * warm-up calls; C is overwritten) and caches the fastest under the
+ * fingerprint; DASPMM_ALG_AUTO then uses it for the same (layout, nv, nr, nnz).
+ * rowIdx may be NULL (COO candidates are then skipped).  Returns the choice
+ * and its time per call in microseconds. */
+daspmm_status daspmm_autotune(int layout, int nr, int nc, int nnz, int nv, const int *rowPtr,
+                              const int *rowIdx, const int *colIdx, const float *values,
+                              const float *B, float *C, int reps, daspmm_config *best,
+                              float *best_us, void *stream);
+/* The cache as a text file (one line per fingerprint), and back. */
+daspmm_status daspmm_tune_save(const char *path);
+daspmm_status daspmm_tune_load(const char *path);
+void daspmm_tune_clear(void);
+
 /* ---- Drop-in for the reference's dispatcher ------------------------------
  * Exactly cudaSpmm<256,32> (spmvspmm.h:53-199): CSR algorithms overwrite C,
  * COO algorithms add into C, the legacy default stream, and the return value
@@ -177,6 +204,49 @@ daspmm_status daspmm_quantize(int fmt, size_t n, const float *x, void *q,
  * scales[k] = max_i |B[i,k]| / 448 (1 for an all-zero column). */
 daspmm_status daspmm_e4m3_scales(int nrows, int ncols, const float *B, float *scales,
                                  void *stream);
+
+/* ---- Batched SpMM (one persistent launch for many problems) --------------
+ * No counterpart in the reference (one problem per cudaSpmm call,
+ * spmvspmm.h:53-199).  Every instance is C = A*B + beta*C with its own CSR A
+ * (nr x nc, nnz), row-major B (nc x nv) and C (nr x nv); all instances of a
+ * batch share nv and the storage formats (values F32 or BF16; B F32, BF16 or
+ * E4M3 with b_scales).  Rows are never split, and each output row is summed
+ * by one warp in nonzero order: a result is bit-identical whatever else is in
+ * the batch.  The device pointers must stay valid while the batch is used. */
+typedef struct daspmm_instance {
+    int nr, nc, nnz, nv;
+    const int *rowPtr;
+    const int *colIdx;
+    const void *values;
+    int val_fmt;
+    const void *B;
+    int b_fmt;
+    const float *b_scales;
+    float *C;
+    float beta;
+} daspmm_instance;
+
+typedef struct daspmm_batch_s *daspmm_batch;
+
+/* Builds the work items ((instance, row tile, column tile), row tiles of
+ * about cfg->chunk nonzeros, default 256) on the device; synchronises
+ * `stream`.  cfg may be NULL. */
+daspmm_status daspmm_batch_create(const daspmm_instance *inst, int n, const daspmm_config *cfg,
+                                  daspmm_batch *out, void *stream);
+/* One queue reset (memset) and one persistent kernel launch on `stream`. */
+daspmm_status daspmm_batch_run(daspmm_batch b, void *stream);
+/* Captures daspmm_batch_run on `stream` (not the legacy stream) into a CUDA
+ * graph kept in the batch; daspmm_batch_replay launches it. */
+daspmm_status daspmm_batch_capture(daspmm_batch b, void *stream);
+daspmm_status daspmm_batch_replay(daspmm_batch b, void *stream);
+daspmm_status daspmm_batch_info(daspmm_batch b, long long *nitems, long long *total_nnz);
+daspmm_status daspmm_batch_destroy(daspmm_batch b);
+/* Autotunes the batch's row-tile size: times daspmm_batch_run for each
+ * chunk in chunks[0..nchunks) (NULL: 128, 256, 512, 1024), reps runs each,
+ * and returns the fastest (C of every instance is overwritten). */
+daspmm_status daspmm_batch_tune(const daspmm_instance *inst, int n, const int *chunks,
+                                int nchunks, int reps, int *best_chunk, float *best_us,
+                                void *stream);
 
 /* ---- Host buffers ------------------------------------------------------
  * The same product with A, B and C in HOST memory (pinned or pageable): the

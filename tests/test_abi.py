@@ -124,3 +124,22 @@ def test_powerlaw_full_size_matches_spec():
     p = D.gen_powerlaw(262144, seed=0)
     assert 1_150_000 < p.nnz < 1_300_000
     assert np.diff(p.rowPtr).max() <= 4096
+
+
+def test_autotune_cache_file_on_host(tmp_path):
+    """A cache file drives DASPMM_ALG_AUTO without any device work."""
+    L = D.lib()
+    L.daspmm_tune_clear()
+    p = tmp_path / "tune.txt"
+    # layout nv dtype nr nnz p50 p90 p99 max us | alg vec L S cf chunk snap block pipe
+    p.write_text("# daspmm autotune cache v1\n"
+                 "0 128 0 5000 60000 7 31 127 900 12.500 1 4 8 4 1 0 0 256 1\n")
+    assert L.daspmm_tune_load(str(p).encode()) == 0
+    c = D.default_config(D.Alg.AUTO, 0, 5000, 5000, 60000, 128)
+    assert (c.alg, c.vec, c.lanes_col, c.lanes_nnz) == (1, 4, 8, 4)
+    c2 = D.default_config(D.Alg.AUTO, 0, 5001, 5001, 60000, 128)   # untuned: rule of thumb
+    assert c2.alg == 4
+    out = tmp_path / "out.txt"
+    assert L.daspmm_tune_save(str(out).encode()) == 0
+    assert "0 128 0 5000 60000" in out.read_text()
+    L.daspmm_tune_clear()
