@@ -322,6 +322,7 @@ def run_ours(args):
             e2e = run_e2e(D, A, B, dev, alg, min(K, args.e2e_steps))
         mixed = None if args.no_mixed else run_mixed(D, A, dA, B, dev, K, peak)
         batched = None if (args.no_batched or world > 1) else run_batched(D, dev)
+        serving = None if (args.no_serving or world > 1) else run_serving(D, dev, args.serve_seconds)
         clk = sampler.summary()
         clk_in = sampler.summary(t0, t1)
         clocks = {"sm_mhz": clk_in["sm_mhz"] if clk_in["samples"] else clk["sm_mhz"],
@@ -347,7 +348,7 @@ def run_ours(args):
                          "peak_source": peak_src},
             "step_hbm_gbs": round(abytes / (ms_step * 1e-3) / 1e9, 1),
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": int(launches),
-            "mixed": mixed, "batched": batched,
+            "mixed": mixed, "batched": batched, "serving": serving,
         }
     if pg:
         pg.barrier()
@@ -472,6 +473,75 @@ def run_batched(D, dev, reps: int = 20):
             "speedup_vs_plain_graph": round(ms_g / ms_b, 3)}
 
 
+def run_serving(D, dev, seconds: float = 1.0, rate: float = 20000.0):
+    """The serving configuration: a pool of 64 resident matrices (rows
+    log-uniform in [1k, 262k], half uniform-random, half power-law), requests
+    with N drawn from {16, 64, 256}, Poisson arrivals at `rate` per second
+    (seed 0).  Served with continuous batching (FP32 values, BF16 B, FP32
+    accumulate) and, as the baseline, one plain FP32 launch per request; both
+    through the same native server (queue, HBM-budget admission, dispatcher
+    thread).  Also the capacity of each: every request queued at t = 0."""
+    import numpy as np
+    import torch
+    import daspmm.workloads as WL
+    pool = WL.config5_pool(64)
+    rng = np.random.default_rng(0)
+    nvs = (16, 64, 256)
+    dmats = [D.DeviceCsr(A, dev) for A in pool]
+    touched = [A.cols_touched() for A in pool]
+    g = torch.Generator(device=dev)
+    g.manual_seed(0)
+    B32, B16 = {}, {}
+    for i, A in enumerate(pool):
+        for nv in nvs:
+            b = torch.empty(A.nc * nv, device=dev).uniform_(-1, 1, generator=g)
+            B32[i, nv] = b
+            B16[i, nv] = D.quantize(b, D.Fmt.BF16)
+    n = int(rate * seconds)
+    arrivals = WL.poisson_arrivals(rate, n, seed=0)
+    pick = rng.integers(0, len(pool), n)
+    pnv = rng.choice(nvs, n)
+    flop = sum(2.0 * pool[m].nnz * int(v) for m, v in zip(pick, pnv))
+
+    def bytes_of(m, nv, s_b):
+        A = pool[m]
+        return A.nnz * 8 + 4 * (A.nr + 1) + touched[m] * nv * s_b + A.nr * nv * 4
+
+    def run(mode, b_fmt, Bs, s_b, arr):
+        srv = D.Server(budget_bytes=8 << 30, mode=mode, b_fmt=b_fmt)
+        ids = [srv.add_matrix(dA) for dA in dmats]
+        reqs = [(ids[m], int(v), Bs[int(m), int(v)]) for m, v in zip(pick, pnv)]
+        srv.replay(reqs[:200], np.zeros(200), release=True)       # warm-up
+        res = srv.replay(reqs, arr, release=True)
+        st = srv.stats()
+        srv.close()
+        lat = np.array([r.latency_us for r in res])
+        ok = sum(r.status == 0 for r in res)
+        span = float(np.max(arr + lat * 1e-6))
+        nbytes = sum(bytes_of(int(m), int(v), s_b) for m, v in zip(pick, pnv))
+        return {"req_s": round(ok / span, 1), "gflops": round(flop / span / 1e9, 1),
+                "gbs": round(nbytes / span / 1e9, 1),
+                "p50_us": round(float(np.percentile(lat, 50)), 1),
+                "p99_us": round(float(np.percentile(lat, 99)), 1),
+                "completed": int(ok), "groups": int(st["groups"]),
+                "mean_group": round(st["launched"] / max(1, st["groups"]), 2),
+                "max_group": int(st["max_group"])}
+
+    out = {"pool": len(pool), "requests": n, "offered_req_s": rate, "nv": list(nvs),
+           "pool_nnz": int(sum(A.nnz for A in pool)),
+           "batched_bf16": run(D.ServeMode.BATCHED, D.Fmt.BF16, B16, 2, arrivals),
+           "plain_fp32": run(D.ServeMode.PLAIN, D.Fmt.F32, B32, 4, arrivals)}
+    zero = np.zeros(n)
+    cap_b = run(D.ServeMode.BATCHED, D.Fmt.BF16, B16, 2, zero)
+    cap_p = run(D.ServeMode.PLAIN, D.Fmt.F32, B32, 4, zero)
+    out["capacity"] = {"batched_bf16_req_s": cap_b["req_s"], "plain_fp32_req_s": cap_p["req_s"],
+                       "batched_bf16_gflops": cap_b["gflops"],
+                       "plain_fp32_gflops": cap_p["gflops"],
+                       "batched_mean_group": cap_b["mean_group"],
+                       "ratio": round(cap_b["req_s"] / max(cap_p["req_s"], 1e-9), 3)}
+    return out
+
+
 def run_e2e(D, A, B, dev, alg, steps):
     """Same SpMM through daspmm_spmm_host: pinned host A, B in; C out."""
     import numpy as np
@@ -519,6 +589,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=1.0)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

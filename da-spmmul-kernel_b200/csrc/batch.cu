@@ -1,15 +1,18 @@
 // batch.cu -- many SpMMs of uneven sizes in one persistent launch.
 //
 // The reference runs one problem per cudaSpmm call (spmvspmm.h:53-199); a
-// batch here is a table of instances (each its own CSR A, dense B and C, all
-// with the same column count nv and storage formats).  A plan kernel cuts
-// every instance into work items -- (instance, row tile, column tile) --
-// where row tiles hold about `chunk` nonzeros and never split a row.  The
-// persistent kernel's warps take items from a device queue (one atomic per
-// item) and gather each item's rows like the lean balanced kernel: windows
-// of 32 nonzeros, four B rows in flight, row ends from a lane cache.  Every
-// output row is summed by one warp in nonzero order, so a result does not
-// depend on what else is in the batch or on scheduling.
+// batch here is a table of instances (each its own CSR A, dense B and C and
+// column count nv; all with the same storage formats).  Every matrix is cut
+// once into tiles of about `chunk` nonzeros (build_tiles): runs of whole rows,
+// and pieces of rows longer than `chunk`, so no work item is longer than one
+// chunk whatever the row-length distribution.  A plan kernel lists the work
+// items -- (instance, tile, column tile) -- and the persistent kernel's warps
+// take them from a device queue (one atomic per item).  A run of rows is
+// gathered like the lean balanced kernel (windows of 32 nonzeros, four B rows
+// in flight, row ends from a lane cache); a piece stores its partial sum in a
+// slot and the row's last piece to finish adds the slots in piece order.
+// A result therefore depends only on its own instance (matrix, nv, chunk),
+// never on the rest of the batch or on scheduling.
 //
 // daspmm_batch_run is one memset (the queue head) and one launch, so it can
 // be captured into a CUDA graph (daspmm_batch_capture / _replay).
@@ -25,30 +28,10 @@
 
 namespace daspmm {
 
-struct BatchInst {
-    int nr, nc, nnz, nv;
-    int ldb, ldc;
-    int row_tiles;  // T = max(1, ceil(nnz / chunk))
-    int col_tiles;  // ceil(nv / W)
-    const int *rowPtr;
-    const int *colIdx;
-    const void *vals;
-    const void *B;
-    const float *bscale;
-    float *C;
-    float beta;
-};
-
-struct BatchItem {
-    int inst, row0, row1, ctile;
-};
-
-// item g -> (instance, row tile t, column tile); row tile t starts at the row
-// holding nonzero t*chunk (row 0 for t = 0) and ends where tile t+1 starts
-// (nr for the last), so tiles cover every row exactly once.
+// item g -> (instance, tile, column tile).
 static __global__ void k_batch_plan(const BatchInst *__restrict__ inst,
                                     const long long *__restrict__ item_begin, int ninst,
-                                    int chunk, BatchItem *items, long long nitems)
+                                    BatchItem *items, long long nitems)
 {
     const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= nitems) return;
@@ -58,26 +41,13 @@ static __global__ void k_batch_plan(const BatchInst *__restrict__ inst,
         if (item_begin[mid] <= g) lo = mid;
         else hi = mid;
     }
-    const BatchInst I = inst[lo];
+    const int ct_n = inst[lo].col_tiles;
     const long long local = g - item_begin[lo];
-    const int t = (int)(local / I.col_tiles), ct = (int)(local % I.col_tiles);
-    auto row_start = [&](int tt) -> int {
-        if (tt == 0) return 0;
-        if (tt >= I.row_tiles) return I.nr;
-        const int k = tt * chunk;  // < nnz: the row containing nonzero k
-        int a = 0, b = I.nr;       // last r with rowPtr[r] <= k
-        while (b - a > 1) {
-            const int m = (a + b) / 2;
-            if (__ldg(I.rowPtr + m) <= k) a = m;
-            else b = m;
-        }
-        return a;
-    };
     BatchItem it;
     it.inst = lo;
-    it.row0 = row_start(t);
-    it.row1 = row_start(t + 1);
-    it.ctile = ct;
+    it.tile = (int)(local / ct_n);
+    it.ctile = (int)(local % ct_n);
+    it.pad_ = 0;
     items[g] = it;
 }
 
@@ -177,7 +147,102 @@ __device__ __forceinline__ void batch_rows(const BatchInst &I, int row0, int row
     }
 }
 
+// One piece (nonzeros [k0, k1) of row row0) for column tile [tb0, tb0 + W):
+// the partial sum goes to the piece's slot; the row's last piece to arrive
+// adds all slots in piece order, scales, applies beta and stores the row.
+template <int W, int U, typename TV, typename TB>
+__device__ __noinline__ void batch_piece(const BatchInst &I, const BatchTile &T, int ct,
+                                            uint64_t pol_once)
+{
+    constexpr int VL = W / 32;
+    constexpr bool SCALED = std::is_same<TB, fp8>::value;
+    const int lane = threadIdx.x & 31;
+    const int col = ct * W + lane * VL;
+    const bool active = col < I.nv;
+    const int colc = active ? col : I.nv - VL;
+    const TB *Bl = reinterpret_cast<const TB *>(I.B) + colc;
+    const TV *Av = reinterpret_cast<const TV *>(I.vals);
+    float acc[VL];
+#pragma unroll
+    for (int e = 0; e < VL; ++e) acc[e] = 0.0f;
+    for (int wb = T.k0; wb < T.k1; wb += 32) {
+        const bool ok = wb + lane < T.k1;
+        const int cl = ok ? ld_hint_s32(I.colIdx + wb + lane, pol_once) : 0;
+        const float vl = ok ? ld_val<TV>(Av + wb + lane, pol_once) : 0.0f;
+        const int cnt = min(32, T.k1 - wb);
+        int t = 0;
+        for (; t + U <= cnt; t += U) {
+            float b[U][VL];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                ld_b<TB, VL>(b[u], Bl + (size_t)__shfl_sync(kFull, cl, t + u) * I.ldb);
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const float v = __shfl_sync(kFull, vl, t + u);
+#pragma unroll
+                for (int e = 0; e < VL; ++e) acc[e] = fmaf(v, b[u][e], acc[e]);
+            }
+        }
+        for (; t < cnt; ++t) {
+            float b[VL];
+            ld_b<TB, VL>(b, Bl + (size_t)__shfl_sync(kFull, cl, t) * I.ldb);
+            const float v = __shfl_sync(kFull, vl, t);
+#pragma unroll
+            for (int e = 0; e < VL; ++e) acc[e] = fmaf(v, b[e], acc[e]);
+        }
+    }
+    float part[VL];
+#pragma unroll
+    for (int e = 0; e < VL; ++e) part[e] = acc[e];
+    float *slot0 = I.slots + (size_t)T.slot * I.nv + col;
+    if (active) st_v<VL>(slot0 + (size_t)T.piece * I.nv, part);
+    __threadfence();
+    __syncwarp();
+    int *counter = I.cnt + (size_t)T.cnt * I.col_tiles + ct;
+    int last = 0;
+    if (lane == 0) last = atomicAdd(counter, 1) == T.npieces - 1;
+    last = __shfl_sync(kFull, last, 0);
+    if (!last) return;
+    __threadfence();
+    if (lane == 0) *counter = 0;  // every piece has arrived: ready for the next run
+    if (!active) return;
+    float tot[VL];
+#pragma unroll
+    for (int e = 0; e < VL; ++e) tot[e] = 0.0f;
+    for (int p = 0; p < T.npieces; ++p) {
+        float h[VL];
+        if (p == T.piece) {
+#pragma unroll
+            for (int e = 0; e < VL; ++e) h[e] = part[e];
+        } else {
+            ld_cg<VL>(h, slot0 + (size_t)p * I.nv);
+        }
+#pragma unroll
+        for (int e = 0; e < VL; ++e) tot[e] += h[e];
+    }
+    float *dst = I.C + (size_t)T.row0 * I.ldc + col;
+#pragma unroll
+    for (int e = 0; e < VL; ++e) tot[e] *= SCALED ? __ldg(I.bscale + col + e) : 1.0f;
+    if (I.beta != 0.0f) {
+        float old[VL];
+        ld_plain<VL>(old, dst);
+#pragma unroll
+        for (int e = 0; e < VL; ++e) tot[e] = fmaf(I.beta, old[e], tot[e]);
+    }
+    st_v<VL>(dst, tot);
+}
+
 template <int W, typename TV, typename TB>
+__device__ __forceinline__ void batch_item(const BatchInst &I, const BatchTile &T, int ct,
+                                           uint64_t pol_once)
+{
+    if (T.piece < 0) batch_rows<W, DASPMM_LEAN_U, TV, TB>(I, T.row0, T.row1, ct * W, pol_once);
+    else batch_piece<W, DASPMM_LEAN_U, TV, TB>(I, T, ct, pol_once);
+}
+
+// WM: the tile width every instance uses, or 0 for a batch of mixed widths
+// (a warp-uniform switch on the item's instance).
+template <int WM, typename TV, typename TB>
 __global__ void __launch_bounds__(256, DASPMM_LEAN_MINB)
     k_batch_spmm(const BatchInst *__restrict__ inst, const BatchItem *__restrict__ items,
                  long long nitems, unsigned long long *head)
@@ -190,9 +255,145 @@ __global__ void __launch_bounds__(256, DASPMM_LEAN_MINB)
         g = __shfl_sync(kFull, g, 0);
         if (g >= (unsigned long long)nitems) return;
         const BatchItem it = items[g];
-        const BatchInst I = inst[it.inst];
-        batch_rows<W, DASPMM_LEAN_U, TV, TB>(I, it.row0, it.row1, it.ctile * W, pol_once);
+        const BatchInst &I = inst[it.inst];  // fields read on use (L1-resident)
+        const BatchTile T = I.tiles[it.tile];
+        if constexpr (WM != 0) {
+            batch_item<WM, TV, TB>(I, T, it.ctile, pol_once);
+        } else {
+            if (I.W == 128) batch_item<128, TV, TB>(I, T, it.ctile, pol_once);
+            else if (I.W == 64) batch_item<64, TV, TB>(I, T, it.ctile, pol_once);
+            else batch_item<32, TV, TB>(I, T, it.ctile, pol_once);
+        }
     }
+}
+
+size_t fmt_size(int f) { return f == DASPMM_F32 ? 4 : (f == DASPMM_E4M3 ? 1 : 2); }
+
+template <int WM, typename TV, typename TB>
+void launch_batch_w(const BatchInst *d_inst, const BatchItem *d_items, long long nitems,
+                    unsigned long long *d_head, cudaStream_t st)
+{
+    const unsigned grid = (unsigned)std::max<long long>(
+        1, std::min<long long>((long long)device_sms() * DASPMM_LEAN_MINB, (nitems + 7) / 8));
+    k_batch_spmm<WM, TV, TB><<<grid, 256, 0, st>>>(d_inst, d_items, nitems, d_head);
+}
+
+template <typename TV, typename TB>
+void launch_batch_t(int wmode, const BatchInst *d_inst, const BatchItem *d_items,
+                    long long nitems, unsigned long long *d_head, cudaStream_t st)
+{
+    if (wmode == 128) launch_batch_w<128, TV, TB>(d_inst, d_items, nitems, d_head, st);
+    else if (wmode == 64) launch_batch_w<64, TV, TB>(d_inst, d_items, nitems, d_head, st);
+    else if (wmode == 32) launch_batch_w<32, TV, TB>(d_inst, d_items, nitems, d_head, st);
+    else launch_batch_w<0, TV, TB>(d_inst, d_items, nitems, d_head, st);
+}
+
+int batch_tile_width(int nv) { return nv % 128 == 0 ? 128 : (nv % 64 == 0 ? 64 : 32); }
+
+bool batch_formats_ok(int vf, int bf)
+{
+    return (vf == DASPMM_F32 && bf == DASPMM_F32) || (vf == DASPMM_F32 && bf == DASPMM_BF16) ||
+           (vf == DASPMM_BF16 && bf == DASPMM_BF16) || (vf == DASPMM_F32 && bf == DASPMM_E4M3) ||
+           (vf == DASPMM_BF16 && bf == DASPMM_E4M3);
+}
+
+daspmm_status batch_fill(const daspmm_instance &s, BatchInst *d)
+{
+    if (s.nv < 1 || s.nr < 0 || s.nc < 0 || s.nnz < 0) return DASPMM_ERR_INVALID;
+    const int W = batch_tile_width(s.nv), VL = W / 32;
+    if (s.nv % VL != 0 || (s.nr > 0 && (!s.rowPtr || !s.C)) ||
+        (s.nnz > 0 && (!s.colIdx || !s.values || !s.B)) ||
+        (s.b_fmt == DASPMM_E4M3 && s.nr > 0 && !s.b_scales) ||
+        ((uintptr_t)s.B % (VL * fmt_size(s.b_fmt))) || ((uintptr_t)s.C % (VL * 4)))
+        return DASPMM_ERR_INVALID;
+    *d = BatchInst{};
+    d->nr = s.nr; d->nc = s.nc; d->nnz = s.nnz; d->nv = s.nv;
+    d->ldb = s.nv; d->ldc = s.nv;
+    d->W = W;
+    d->col_tiles = (s.nv + W - 1) / W;
+    d->rowPtr = s.rowPtr; d->colIdx = s.colIdx; d->vals = s.values; d->B = s.B;
+    d->bscale = s.b_scales; d->C = s.C; d->beta = s.beta;
+    return DASPMM_OK;
+}
+
+void build_tiles(const int *rp, int nr, int chunk, TilePlan *out)
+{
+    out->tiles.clear();
+    out->npieces = 0;
+    out->nlong = 0;
+    int r = 0;
+    while (r < nr) {
+        const int len = rp[r + 1] - rp[r];
+        if (len > chunk) {  // a long row: pieces of `chunk` nonzeros
+            const int P = (len + chunk - 1) / chunk;
+            for (int p = 0; p < P; ++p) {
+                BatchTile t;
+                t.row0 = r;
+                t.row1 = r + 1;
+                t.k0 = rp[r] + p * chunk;
+                t.k1 = std::min(rp[r + 1], t.k0 + chunk);
+                t.piece = p;
+                t.npieces = P;
+                t.slot = out->npieces;
+                t.cnt = out->nlong;
+                out->tiles.push_back(t);
+            }
+            out->npieces += P;
+            ++out->nlong;
+            ++r;
+            continue;
+        }
+        // a run of short rows: nonzeros + rows (each row costs a store) <= chunk
+        BatchTile t{};
+        t.row0 = r;
+        t.piece = -1;
+        long long cost = 0;
+        while (r < nr) {
+            const int l = rp[r + 1] - rp[r];
+            if (l > chunk || (r > t.row0 && cost + l + 1 > chunk)) break;
+            cost += l + 1;
+            ++r;
+        }
+        t.row1 = r;
+        t.k0 = rp[t.row0];
+        t.k1 = rp[r];
+        out->tiles.push_back(t);
+    }
+}
+
+daspmm_status batch_plan_async(const BatchInst *d_inst, const long long *d_begin, int n,
+                               BatchItem *d_items, long long nitems, cudaStream_t st)
+{
+    if (nitems <= 0) return DASPMM_OK;
+    const unsigned g = (unsigned)((nitems + 255) / 256);
+    k_batch_plan<<<g, 256, 0, st>>>(d_inst, d_begin, n, d_items, nitems);
+    count_launches(1);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? DASPMM_OK : cuda_fail(e);
+}
+
+daspmm_status batch_kernel_async(int vf, int bf, int wmode, const BatchInst *d_inst,
+                                 const BatchItem *d_items, long long nitems,
+                                 unsigned long long *d_head, cudaStream_t st)
+{
+    if (nitems <= 0) return DASPMM_OK;
+    cudaError_t e = cudaMemsetAsync(d_head, 0, sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return cuda_fail(e);
+    timer_before(st);
+    if (vf == DASPMM_F32 && bf == DASPMM_F32)
+        launch_batch_t<float, float>(wmode, d_inst, d_items, nitems, d_head, st);
+    else if (vf == DASPMM_F32 && bf == DASPMM_BF16)
+        launch_batch_t<float, bf16>(wmode, d_inst, d_items, nitems, d_head, st);
+    else if (vf == DASPMM_BF16 && bf == DASPMM_BF16)
+        launch_batch_t<bf16, bf16>(wmode, d_inst, d_items, nitems, d_head, st);
+    else if (vf == DASPMM_F32 && bf == DASPMM_E4M3)
+        launch_batch_t<float, fp8>(wmode, d_inst, d_items, nitems, d_head, st);
+    else
+        launch_batch_t<bf16, fp8>(wmode, d_inst, d_items, nitems, d_head, st);
+    timer_after(st);
+    count_launches(1);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? DASPMM_OK : cuda_fail(e);
 }
 
 }  // namespace daspmm
@@ -206,6 +407,9 @@ struct daspmm_batch_s {
     BatchInst *d_inst = nullptr;
     long long *d_begin = nullptr;
     BatchItem *d_items = nullptr;
+    BatchTile *d_tiles = nullptr;
+    float *d_slots = nullptr;
+    int *d_cnt = nullptr;
     unsigned long long *d_head = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -213,36 +417,10 @@ struct daspmm_batch_s {
 
 namespace {
 
-template <int W, typename TV, typename TB>
-void launch_batch_w(daspmm_batch_s *b, cudaStream_t st)
-{
-    const unsigned grid = (unsigned)std::max<long long>(
-        1, std::min<long long>((long long)device_sms() * DASPMM_LEAN_MINB, (b->nitems + 7) / 8));
-    k_batch_spmm<W, TV, TB><<<grid, 256, 0, st>>>(b->d_inst, b->d_items, b->nitems, b->d_head);
-}
-
-template <typename TV, typename TB>
-void launch_batch_t(daspmm_batch_s *b, cudaStream_t st)
-{
-    if (b->W == 128) launch_batch_w<128, TV, TB>(b, st);
-    else if (b->W == 64) launch_batch_w<64, TV, TB>(b, st);
-    else launch_batch_w<32, TV, TB>(b, st);
-}
-
 daspmm_status batch_launch(daspmm_batch_s *b, cudaStream_t st)
 {
-    cudaError_t e = cudaMemsetAsync(b->d_head, 0, sizeof(unsigned long long), st);
-    if (e != cudaSuccess) return cuda_fail(e);
-    timer_before(st);
-    if (b->val_fmt == DASPMM_F32 && b->b_fmt == DASPMM_F32) launch_batch_t<float, float>(b, st);
-    else if (b->val_fmt == DASPMM_F32 && b->b_fmt == DASPMM_BF16) launch_batch_t<float, bf16>(b, st);
-    else if (b->val_fmt == DASPMM_BF16 && b->b_fmt == DASPMM_BF16) launch_batch_t<bf16, bf16>(b, st);
-    else if (b->val_fmt == DASPMM_F32 && b->b_fmt == DASPMM_E4M3) launch_batch_t<float, fp8>(b, st);
-    else launch_batch_t<bf16, fp8>(b, st);
-    timer_after(st);
-    count_launches(1);
-    e = cudaGetLastError();
-    return e == cudaSuccess ? DASPMM_OK : cuda_fail(e);
+    return batch_kernel_async(b->val_fmt, b->b_fmt, b->W, b->d_inst, b->d_items, b->nitems,
+                              b->d_head, st);
 }
 
 void batch_free(daspmm_batch_s *b)
@@ -252,11 +430,12 @@ void batch_free(daspmm_batch_s *b)
     cudaFree(b->d_inst);
     cudaFree(b->d_begin);
     cudaFree(b->d_items);
+    cudaFree(b->d_tiles);
+    cudaFree(b->d_slots);
+    cudaFree(b->d_cnt);
     cudaFree(b->d_head);
     delete b;
 }
-
-size_t fmt_size(int f) { return f == DASPMM_F32 ? 4 : (f == DASPMM_E4M3 ? 1 : 2); }
 
 }  // namespace
 
@@ -278,40 +457,63 @@ daspmm_status daspmm_batch_create(const daspmm_instance *inst, int n, const dasp
         b->val_fmt = inst[0].val_fmt;
         b->b_fmt = inst[0].b_fmt;
     }
-    const bool combo = (b->val_fmt == DASPMM_F32 && b->b_fmt == DASPMM_F32) ||
-                       (b->val_fmt == DASPMM_F32 && b->b_fmt == DASPMM_BF16) ||
-                       (b->val_fmt == DASPMM_BF16 && b->b_fmt == DASPMM_BF16) ||
-                       (b->val_fmt == DASPMM_F32 && b->b_fmt == DASPMM_E4M3) ||
-                       (b->val_fmt == DASPMM_BF16 && b->b_fmt == DASPMM_E4M3);
-    if (n > 0 && (!combo || b->nv < 1)) {
+    if (n > 0 && !batch_formats_ok(b->val_fmt, b->b_fmt)) {
         delete b;
         return DASPMM_ERR_UNSUPPORTED;
     }
-    // tile width: the widest of 128 / 64 / 32 dividing nv, else 32 (lanes masked)
-    const int nv = std::max(1, b->nv);
-    b->W = nv % 128 == 0 ? 128 : (nv % 64 == 0 ? 64 : 32);
-    const int VL = b->W / 32;
     std::vector<BatchInst> hi(n);
-    std::vector<long long> begin(n + 1, 0);
     for (int i = 0; i < n; ++i) {
         const daspmm_instance &s = inst[i];
-        if (s.nv != b->nv || s.val_fmt != b->val_fmt || s.b_fmt != b->b_fmt || s.nr < 0 ||
-            s.nc < 0 || s.nnz < 0 || s.nv % VL != 0 || (s.nr > 0 && (!s.rowPtr || !s.C)) ||
-            (s.nnz > 0 && (!s.colIdx || !s.values || !s.B)) ||
-            (s.b_fmt == DASPMM_E4M3 && !s.b_scales) ||
-            ((uintptr_t)s.B % (VL * fmt_size(s.b_fmt))) || ((uintptr_t)s.C % (VL * 4))) {
+        const daspmm_status fs = (s.val_fmt != b->val_fmt || s.b_fmt != b->b_fmt)
+                                     ? DASPMM_ERR_INVALID
+                                     : batch_fill(s, &hi[i]);
+        if (fs != DASPMM_OK) {
             delete b;
-            return DASPMM_ERR_INVALID;
+            return fs;
         }
-        BatchInst &d = hi[i];
-        d.nr = s.nr; d.nc = s.nc; d.nnz = s.nnz; d.nv = s.nv;
-        d.ldb = s.nv; d.ldc = s.nv;
-        d.row_tiles = s.nr == 0 ? 0 : (int)std::max<long long>(1, ((long long)s.nnz + b->chunk - 1) / b->chunk);
-        d.col_tiles = (s.nv + b->W - 1) / b->W;
-        d.rowPtr = s.rowPtr; d.colIdx = s.colIdx; d.vals = s.values; d.B = s.B;
-        d.bscale = s.b_scales; d.C = s.C; d.beta = s.beta;
-        begin[i + 1] = begin[i] + (long long)d.row_tiles * d.col_tiles;
+        const int w = hi[i].W;
+        b->W = (i == 0 || b->W == w) ? w : 0;  // 0: widths differ
         b->total_nnz += s.nnz;
+    }
+    // Tiles from each rowPtr (copied to the host once).
+    std::vector<BatchTile> tiles;
+    std::vector<size_t> tile_off(n), slot_off(n), cnt_off(n);
+    size_t nslot = 0, ncnt = 0;
+    std::vector<long long> begin(n + 1, 0);
+    {
+        std::vector<int> rp;
+        TilePlan plan;
+        for (int i = 0; i < n; ++i) {
+            const daspmm_instance &s = inst[i];
+            rp.resize((size_t)s.nr + 1);
+            if (s.nr > 0) {
+                const cudaError_t e = cudaMemcpyAsync(rp.data(), s.rowPtr, sizeof(int) * (s.nr + 1),
+                                                      cudaMemcpyDeviceToHost, st);
+                const cudaError_t e2 = e == cudaSuccess ? cudaStreamSynchronize(st) : e;
+                if (e2 != cudaSuccess) {
+                    delete b;
+                    return cuda_fail(e2);
+                }
+                if (rp[0] != 0 || rp[s.nr] != s.nnz) {
+                    delete b;
+                    return DASPMM_ERR_BAD_MATRIX;
+                }
+                for (int r = 0; r < s.nr; ++r)
+                    if (rp[r + 1] < rp[r]) {
+                        delete b;
+                        return DASPMM_ERR_BAD_MATRIX;
+                    }
+            }
+            build_tiles(rp.data(), s.nr, b->chunk, &plan);
+            tile_off[i] = tiles.size();
+            slot_off[i] = nslot;
+            cnt_off[i] = ncnt;
+            tiles.insert(tiles.end(), plan.tiles.begin(), plan.tiles.end());
+            nslot += (size_t)plan.npieces * s.nv;
+            ncnt += (size_t)plan.nlong * hi[i].col_tiles;
+            hi[i].ntiles = (int)plan.tiles.size();
+            begin[i + 1] = begin[i] + (long long)hi[i].ntiles * hi[i].col_tiles;
+        }
     }
     b->nitems = begin[n];
     cudaError_t e = cudaSuccess;
@@ -319,22 +521,37 @@ daspmm_status daspmm_batch_create(const daspmm_instance *inst, int n, const dasp
     if (e == cudaSuccess && n) e = cudaMalloc(&b->d_inst, sizeof(BatchInst) * n);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_begin, sizeof(long long) * (n + 1));
     if (e == cudaSuccess && b->nitems) e = cudaMalloc(&b->d_items, sizeof(BatchItem) * b->nitems);
+    if (e == cudaSuccess && !tiles.empty()) e = cudaMalloc(&b->d_tiles, sizeof(BatchTile) * tiles.size());
+    if (e == cudaSuccess && nslot) e = cudaMalloc(&b->d_slots, sizeof(float) * nslot);
+    if (e == cudaSuccess && ncnt) e = cudaMalloc(&b->d_cnt, sizeof(int) * ncnt);
     if (e != cudaSuccess) {
         cudaGetLastError();
         batch_free(b);
         return DASPMM_ERR_NOMEM;
     }
-    if (n) e = cudaMemcpyAsync(b->d_inst, hi.data(), sizeof(BatchInst) * n, cudaMemcpyHostToDevice, st);
+    for (int i = 0; i < n; ++i) {
+        hi[i].tiles = b->d_tiles ? b->d_tiles + tile_off[i] : nullptr;
+        hi[i].slots = b->d_slots ? b->d_slots + slot_off[i] : nullptr;
+        hi[i].cnt = b->d_cnt ? b->d_cnt + cnt_off[i] : nullptr;
+    }
+    if (ncnt) e = cudaMemsetAsync(b->d_cnt, 0, sizeof(int) * ncnt, st);
+    if (e == cudaSuccess && !tiles.empty())
+        e = cudaMemcpyAsync(b->d_tiles, tiles.data(), sizeof(BatchTile) * tiles.size(),
+                            cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && n)
+        e = cudaMemcpyAsync(b->d_inst, hi.data(), sizeof(BatchInst) * n, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(b->d_begin, begin.data(), sizeof(long long) * (n + 1),
                             cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess && b->nitems) {
-        const unsigned g = (unsigned)((b->nitems + 255) / 256);
-        k_batch_plan<<<g, 256, 0, st>>>(b->d_inst, b->d_begin, n, b->chunk, b->d_items, b->nitems);
-        count_launches(1);
-        e = cudaGetLastError();
+    if (e == cudaSuccess) {
+        const daspmm_status ps =
+            batch_plan_async(b->d_inst, b->d_begin, n, b->d_items, b->nitems, st);
+        if (ps != DASPMM_OK) {
+            batch_free(b);
+            return ps;
+        }
+        e = cudaStreamSynchronize(st);  // host vectors go out of scope
     }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // host vectors go out of scope
     if (e != cudaSuccess) {
         batch_free(b);
         return cuda_fail(e);

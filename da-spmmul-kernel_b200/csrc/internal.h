@@ -7,6 +7,8 @@
 #include <cuda_runtime.h>
 #include <stddef.h>
 
+#include <vector>
+
 namespace daspmm {
 
 // A fully resolved design-space point for one problem shape.
@@ -57,6 +59,73 @@ daspmm_status cached_host_staging(size_t need, cudaStream_t st, void **out);
 void count_launches(int n);
 void timer_before(cudaStream_t st);
 void timer_after(cudaStream_t st);
+
+// Batched SpMM (batch.cu), shared with the serving loop (serve.cu).
+//
+// A matrix is cut once into tiles (build_tiles, on the host from rowPtr):
+// runs of whole rows holding at most `chunk` nonzeros plus rows (counting a
+// row as one unit of work), and every row longer than `chunk` cut into pieces
+// of `chunk` nonzeros.  A piece's partial sum goes to a slot; the last piece
+// of a row to finish adds the row's slots in piece order and stores it, so
+// results are deterministic and depend only on the matrix and `chunk`.
+struct BatchTile {
+    int row0, row1;   // rows [row0, row1); a piece has row1 = row0 + 1
+    int k0, k1;       // piece: nonzeros [k0, k1)
+    int piece;        // -1 for a run of whole rows, else the piece index
+    int npieces;      // pieces of the row
+    int slot;         // piece: slot of piece 0 (slots slot .. slot+npieces-1)
+    int cnt;          // piece: the row's counter index
+};
+
+struct TilePlan {
+    std::vector<BatchTile> tiles;
+    int npieces = 0;  // slots needed (x nv floats)
+    int nlong = 0;    // rows cut into pieces (x column tiles counters)
+};
+
+void build_tiles(const int *rowPtr, int nr, int chunk, TilePlan *out);
+
+// One instance as the persistent kernel sees it.  W is the instance's column
+// tile width (128, 64 or 32 floats, from its own nv only).  slots holds
+// npieces * nv floats, cnt nlong * col_tiles counters that start at zero and
+// are left at zero by the kernel (the last piece resets its row's counter).
+struct BatchInst {
+    int nr, nc, nnz, nv;
+    int ldb, ldc;
+    int ntiles;
+    int col_tiles;  // ceil(nv / W)
+    int W;
+    int pad_;
+    const int *rowPtr;
+    const int *colIdx;
+    const void *vals;
+    const void *B;
+    const float *bscale;
+    float *C;
+    const BatchTile *tiles;
+    float *slots;
+    int *cnt;
+    float beta;
+};
+
+struct BatchItem {
+    int inst, tile, ctile, pad_;
+};
+
+int batch_tile_width(int nv);
+bool batch_formats_ok(int val_fmt, int b_fmt);
+// Checks one instance and fills its kernel-side row except tiles / ntiles /
+// slots / cnt (DASPMM_ERR_INVALID on a bad size, pointer or alignment).
+daspmm_status batch_fill(const daspmm_instance &s, BatchInst *d);
+// item table of n instances whose item counts (ntiles * col_tiles) prefix to
+// d_begin[0..n].
+daspmm_status batch_plan_async(const BatchInst *d_inst, const long long *d_begin, int n,
+                               BatchItem *d_items, long long nitems, cudaStream_t st);
+// Queue reset + one persistent launch.  wmode: the common tile width of all
+// instances (128, 64, 32) or 0 when they differ.
+daspmm_status batch_kernel_async(int val_fmt, int b_fmt, int wmode, const BatchInst *d_inst,
+                                 const BatchItem *d_items, long long nitems,
+                                 unsigned long long *d_head, cudaStream_t st);
 
 // Autotuner (tune.cu): the cached best configuration for a shape, or the
 // library's rule-of-thumb choice when nothing has been measured yet.

@@ -432,6 +432,122 @@ class Batch:
             pass
 
 
+# ---------------------------------------------------------------- validation
+def csr_check(A: DeviceCsr, sorted_cols: bool = False, stream=None) -> int:
+    """-1 when A passes daspmm_csr_check, else the first offending row."""
+    bad = ctypes.c_int(-1)
+    st = _lib().daspmm_csr_check(A.nr, A.nc, A.nnz, _dptr(A.rowPtr), _dptr(A.colIdx),
+                                 int(bool(sorted_cols)), ctypes.byref(bad), _stream_ptr(stream))
+    if st == 9:
+        return bad.value
+    check(st, "csr_check")
+    return -1
+
+
+# ---------------------------------------------------------------- serving
+class ServeMode(enum.IntEnum):
+    BATCHED = 0
+    PLAIN = 1
+
+
+class _DeviceView:
+    """A raw device float32 buffer as a torch tensor (no copy)."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f4",
+                                         "data": (ptr, False), "version": 3, "strides": None}
+
+
+class Server:
+    """daspmm_server_*: a pool of resident matrices, an output arena and a
+    dispatcher thread.  Matrices (DeviceCsr + values tensor) and every
+    request's B must outlive the server's use of them."""
+
+    def __init__(self, budget_bytes: int = 1 << 30, mode: int = ServeMode.BATCHED,
+                 val_fmt: int = Fmt.F32, b_fmt: int = Fmt.F32, chunk: int = 0,
+                 max_batch: int = 0, max_inflight: int = 0, window_us: int = 0,
+                 max_items: int = 0, scratch_bytes: int = 0):
+        from ._sigs import ServerConfig
+        cfg = ServerConfig(int(budget_bytes), int(mode), int(val_fmt), int(b_fmt), chunk,
+                           max_batch, max_inflight, window_us, max_items, scratch_bytes)
+        self._h = ctypes.c_void_p()
+        check(_lib().daspmm_server_create(ctypes.byref(cfg), ctypes.byref(self._h)),
+              "server_create")
+        self._keep = []
+        self.shapes = []
+
+    def add_matrix(self, A: DeviceCsr, values=None) -> int:
+        mid = ctypes.c_int(-1)
+        v = A.values if values is None else values
+        check(_lib().daspmm_server_add_matrix(self._h, A.nr, A.nc, A.nnz, _dptr(A.rowPtr),
+                                              _dptr(A.colIdx), _dptr(v), ctypes.byref(mid)),
+              "server_add_matrix")
+        self._keep.append((A, v))
+        self.shapes.append((A.nr, A.nc, A.nnz))
+        return mid.value
+
+    @staticmethod
+    def _req(matrix: int, nv: int, B, b_scales=None):
+        from ._sigs import Request
+        return Request(int(matrix), int(nv), _dptr(B) or 0, _dptr(b_scales) or 0)
+
+    def submit(self, matrix: int, nv: int, B, b_scales=None) -> int:
+        t = ctypes.c_longlong()
+        r = self._req(matrix, nv, B, b_scales)
+        check(_lib().daspmm_server_submit(self._h, ctypes.byref(r), ctypes.byref(t)),
+              "server_submit")
+        return t.value
+
+    def cancel(self, ticket: int) -> int:
+        return _lib().daspmm_server_cancel(self._h, int(ticket))
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        from ._sigs import Result
+        r = Result()
+        st = _lib().daspmm_server_wait(self._h, int(ticket), int(timeout_ms), ctypes.byref(r))
+        return st, r
+
+    def result_tensor(self, res, nrows: int, nv: int):
+        """The result's C (device, FP32) as a torch tensor view; valid until release."""
+        import torch
+        if not res.C:
+            return None
+        return torch.as_tensor(_DeviceView(res.C, nrows * nv), device="cuda")
+
+    def release(self, ticket: int) -> None:
+        check(_lib().daspmm_server_release(self._h, int(ticket)), "server_release")
+
+    def replay(self, requests, arrivals, release: bool = True):
+        """requests: list of (matrix, nv, B[, b_scales]); arrivals: seconds."""
+        from ._sigs import Request, Result
+        n = len(requests)
+        arr = (Request * max(1, n))()
+        for i, q in enumerate(requests):
+            arr[i] = self._req(*q)
+        ts = (ctypes.c_double * max(1, n))(*[float(a) for a in arrivals])
+        res = (Result * max(1, n))()
+        st = _lib().daspmm_server_replay(self._h, arr, n, ts, int(bool(release)), res)
+        check(st, "server_replay")
+        return [res[i] for i in range(n)]
+
+    def stats(self) -> dict:
+        from ._sigs import ServeStats
+        o = ServeStats()
+        check(_lib().daspmm_server_stats(self._h, ctypes.byref(o)), "server_stats")
+        return {n: getattr(o, n) for n, _ in o._fields_}
+
+    def close(self):
+        if self._h:
+            _lib().daspmm_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # ---------------------------------------------------------------- problem
 class SpmvSpmmProblem:
     """Non-owning view of device buffers with run/benchmark, after

@@ -22,6 +22,35 @@ class Fingerprint(ctypes.Structure):
                                   "max_row")]
 
 
+_LL = ctypes.c_longlong
+_D = ctypes.c_double
+
+
+class ServerConfig(ctypes.Structure):
+    """daspmm_server_config (include/daspmm.h)."""
+    _fields_ = [("budget_bytes", _LL), ("mode", _I), ("val_fmt", _I), ("b_fmt", _I),
+                ("chunk", _I), ("max_batch", _I), ("max_inflight", _I), ("window_us", _I),
+                ("max_items", _LL), ("scratch_bytes", _LL)]
+
+
+class Request(ctypes.Structure):
+    """daspmm_request (include/daspmm.h)."""
+    _fields_ = [("matrix", _I), ("nv", _I), ("B", _VP), ("b_scales", _VP)]
+
+
+class Result(ctypes.Structure):
+    """daspmm_result (include/daspmm.h)."""
+    _fields_ = [("status", _I), ("group", _I), ("C", _VP), ("queue_us", _D),
+                ("latency_us", _D)]
+
+
+class ServeStats(ctypes.Structure):
+    """daspmm_serve_stats (include/daspmm.h)."""
+    _fields_ = [(n, _LL) for n in ("completed", "cancelled", "refused", "groups", "launched",
+                                   "items", "queued", "arena_used", "arena_bytes")] + \
+               [(n, _I) for n in ("max_group", "inflight_groups", "matrices", "error")]
+
+
 def apply(lib, Config):
     sig = {
         "daspmm_batch_create": (_I, [ctypes.POINTER(Instance), _I, ctypes.POINTER(Config),
@@ -50,6 +79,17 @@ def apply(lib, Config):
         "daspmm_quantize": (_I, [_I, ctypes.c_size_t, _VP, _VP, _VP, _I, _VP]),
         "daspmm_e4m3_scales": (_I, [_I, _I, _VP, _VP, _VP]),
         "daspmm_device_error": (_I, []),
+        "daspmm_csr_check": (_I, [_I, _I, _I, _VP, _VP, _I, ctypes.POINTER(_I), _VP]),
+        "daspmm_server_create": (_I, [ctypes.POINTER(ServerConfig), ctypes.POINTER(_VP)]),
+        "daspmm_server_add_matrix": (_I, [_VP, _I, _I, _I, _VP, _VP, _VP, ctypes.POINTER(_I)]),
+        "daspmm_server_submit": (_I, [_VP, ctypes.POINTER(Request), ctypes.POINTER(_LL)]),
+        "daspmm_server_cancel": (_I, [_VP, _LL]),
+        "daspmm_server_wait": (_I, [_VP, _LL, _I, ctypes.POINTER(Result)]),
+        "daspmm_server_release": (_I, [_VP, _LL]),
+        "daspmm_server_replay": (_I, [_VP, ctypes.POINTER(Request), _I, ctypes.POINTER(_D), _I,
+                                      ctypes.POINTER(Result)]),
+        "daspmm_server_stats": (_I, [_VP, ctypes.POINTER(ServeStats)]),
+        "daspmm_server_destroy": (_I, [_VP]),
         "daspmm_kernel_timer_begin": (_I, [_I]),
         "daspmm_kernel_timer_end": (_I, [ctypes.POINTER(ctypes.c_float), _I]),
     }

@@ -208,11 +208,11 @@ daspmm_status daspmm_e4m3_scales(int nrows, int ncols, const float *B, float *sc
 /* ---- Batched SpMM (one persistent launch for many problems) --------------
  * No counterpart in the reference (one problem per cudaSpmm call,
  * spmvspmm.h:53-199).  Every instance is C = A*B + beta*C with its own CSR A
- * (nr x nc, nnz), row-major B (nc x nv) and C (nr x nv); all instances of a
- * batch share nv and the storage formats (values F32 or BF16; B F32, BF16 or
- * E4M3 with b_scales).  Rows are never split, and each output row is summed
- * by one warp in nonzero order: a result is bit-identical whatever else is in
- * the batch.  The device pointers must stay valid while the batch is used. */
+ * (nr x nc, nnz), row-major B (nc x nv) and C (nr x nv); nv may differ
+ * between instances (column tiles of 128, 64 or 32 by each instance's own nv),
+ * the storage formats are the batch's (values F32 or BF16; B F32, BF16 or
+ * E4M3 with b_scales).  How a row is summed depends only on its own matrix,
+ * nv and chunk: a result is bit-identical whatever else is in the batch.  The device pointers must stay valid while the batch is used. */
 typedef struct daspmm_instance {
     int nr, nc, nnz, nv;
     const int *rowPtr;
@@ -228,9 +228,14 @@ typedef struct daspmm_instance {
 
 typedef struct daspmm_batch_s *daspmm_batch;
 
-/* Builds the work items ((instance, row tile, column tile), row tiles of
- * about cfg->chunk nonzeros, default 256) on the device; synchronises
- * `stream`.  cfg may be NULL. */
+/* Cuts every matrix into tiles of about cfg->chunk nonzeros (default 256;
+ * runs of whole rows, and rows longer than chunk cut into pieces of chunk
+ * nonzeros whose partial sums are added in piece order by the row's last
+ * piece), reading each rowPtr once on the host, and lists the work items
+ * (instance, tile, column tile) on the device; synchronises `stream`.
+ * DASPMM_ERR_BAD_MATRIX when a rowPtr is not a valid row pointer.  The batch
+ * keeps scratch for the pieces: one batch must not run on two streams at
+ * once.  cfg may be NULL. */
 daspmm_status daspmm_batch_create(const daspmm_instance *inst, int n, const daspmm_config *cfg,
                                   daspmm_batch *out, void *stream);
 /* One queue reset (memset) and one persistent kernel launch on `stream`. */
@@ -247,6 +252,103 @@ daspmm_status daspmm_batch_destroy(daspmm_batch b);
 daspmm_status daspmm_batch_tune(const daspmm_instance *inst, int n, const int *chunks,
                                 int nchunks, int reps, int *best_chunk, float *best_us,
                                 void *stream);
+
+/* ---- CSR validation -------------------------------------------------------
+ * Checks a device CSR matrix: rowPtr[0] == 0, rowPtr[nr] == nnz, rowPtr
+ * non-decreasing, every colIdx in [0, nc) and, with sorted != 0, strictly
+ * increasing columns inside each row (the driver's order, spmatrix.hpp:327).
+ * Synchronises `stream`.  DASPMM_ERR_BAD_MATRIX with *bad_row = the first
+ * offending row (when bad_row is not NULL; -1 otherwise).  The reference
+ * checks nothing (spmvspmm_benchmark.cu:41-76 trusts a sorted rowIdx). */
+daspmm_status daspmm_csr_check(int nr, int nc, int nnz, const int *rowPtr, const int *colIdx,
+                               int sorted, int *bad_row, void *stream);
+
+/* ---- Serving loop ----------------------------------------------------------
+ * No counterpart in the reference (SpmvSpmmProblem::benchmark times one
+ * problem in a loop, spmvspmm.h:220-243).  A server owns a CUDA stream on
+ * the device current at creation, a pool of device-resident CSR matrices
+ * (caller-owned device arrays, checked once by daspmm_csr_check when added),
+ * an output arena of budget_bytes device bytes and a dispatcher thread.
+ * A request is C = A_m * B (FP32 C, row-major nr x nv, placed in the arena);
+ * B is caller-owned device memory (row-major nc x nv in the server's b_fmt)
+ * that must stay valid until the request finishes.
+ *   admission: requests are launched in FIFO order once their C fits the
+ *     arena; C stays allocated until daspmm_server_release.  A request whose
+ *     C alone exceeds the budget is refused at submission (DASPMM_ERR_BUDGET).
+ *   DASPMM_SERVE_BATCHED: each matrix is cut into tiles once when added (see
+ *     daspmm_batch_create); whenever fewer than max_inflight launch groups are
+ *     in flight, everything queued (up to max_batch requests and max_items
+ *     work items) goes into one persistent batched launch (see daspmm_batch_*);
+ *     with window_us > 0 and the GPU busy, a group is held back until its
+ *     oldest request has waited window_us or max_batch requests are queued.
+ *     A request's result does not depend on which group it lands in.
+ *   DASPMM_SERVE_PLAIN: one daspmm_spmm (balanced CSR, FP32) launch per
+ *     request; val_fmt and b_fmt must be DASPMM_F32.
+ * Latency: from arrival (submission, or the scheduled time in
+ * daspmm_server_replay) to the dispatcher seeing the launch's event. */
+#define DASPMM_SERVE_BATCHED 0
+#define DASPMM_SERVE_PLAIN 1
+
+typedef struct daspmm_server_config {
+    long long budget_bytes;  /* output arena bytes; 0: 1 GiB */
+    int mode;                /* DASPMM_SERVE_BATCHED or DASPMM_SERVE_PLAIN */
+    int val_fmt, b_fmt;      /* storage of every matrix's values / every B */
+    int chunk;               /* batched: nonzeros per row tile; 0: 256 */
+    int max_batch;           /* batched: requests per launch; 0: 1024 */
+    int max_inflight;        /* launch groups in flight; 0: 2 batched, 64 plain */
+    int window_us;           /* batched: batching window while the GPU is busy */
+    long long max_items;     /* batched: work items per launch; 0: 1 << 22 */
+    long long scratch_bytes; /* batched: row-piece sums per launch group; 0: 64 MiB */
+} daspmm_server_config;
+
+typedef struct daspmm_request {
+    int matrix;              /* id from daspmm_server_add_matrix */
+    int nv;
+    const void *B;
+    const float *b_scales;   /* E4M3 B: per-column scales */
+} daspmm_request;
+
+typedef struct daspmm_result {
+    int status;              /* DASPMM_OK, DASPMM_ERR_CANCELLED, ...; -1 pending */
+    int group;               /* launch group that served it (-1: none) */
+    float *C;                /* device result in the arena until released */
+    double queue_us;         /* arrival -> launch */
+    double latency_us;       /* arrival -> completion seen */
+} daspmm_result;
+
+typedef struct daspmm_serve_stats {
+    long long completed, cancelled, refused, groups, launched, items, queued;
+    long long arena_used, arena_bytes;
+    int max_group, inflight_groups, matrices, error;
+} daspmm_serve_stats;
+
+typedef struct daspmm_server_s *daspmm_server;
+
+daspmm_status daspmm_server_create(const daspmm_server_config *cfg, daspmm_server *out);
+/* Adds a resident matrix (device rowPtr/colIdx/values, complete before the
+ * call); DASPMM_ERR_BAD_MATRIX when it fails the CSR check. */
+daspmm_status daspmm_server_add_matrix(daspmm_server s, int nr, int nc, int nnz,
+                                       const int *rowPtr, const int *colIdx,
+                                       const void *values, int *id);
+daspmm_status daspmm_server_submit(daspmm_server s, const daspmm_request *r, long long *ticket);
+/* Removes a request that is still queued (DASPMM_ERR_UNSUPPORTED once it
+ * has been launched); its result reports DASPMM_ERR_CANCELLED. */
+daspmm_status daspmm_server_cancel(daspmm_server s, long long ticket);
+/* Waits for a request (timeout_ms < 0: no limit; DASPMM_ERR_TIMEOUT when it
+ * expires).  The result stays readable until daspmm_server_release. */
+daspmm_status daspmm_server_wait(daspmm_server s, long long ticket, int timeout_ms,
+                                 daspmm_result *out);
+/* Frees a finished request's C and forgets it. */
+daspmm_status daspmm_server_release(daspmm_server s, long long ticket);
+/* Open-loop load from the calling thread: submits reqs[i] at arrival_s[i]
+ * seconds after the call, waits for all and fills results[i] (refused
+ * submissions carry their status).  release != 0 frees every C at once. */
+daspmm_status daspmm_server_replay(daspmm_server s, const daspmm_request *reqs, int n,
+                                   const double *arrival_s, int release,
+                                   daspmm_result *results);
+daspmm_status daspmm_server_stats(daspmm_server s, daspmm_serve_stats *out);
+/* Cancels queued requests, lets launched ones finish, frees everything. */
+daspmm_status daspmm_server_destroy(daspmm_server s);
 
 /* ---- Host buffers ------------------------------------------------------
  * The same product with A, B and C in HOST memory (pinned or pageable): the
