@@ -229,10 +229,18 @@ def run_ours(args):
     L = D.lib()
     alg = D.Alg[args.alg]
 
-    A = D.gen_powerlaw(NR, seed=rank)           # this rank's row shard
-    B = D.gen_dense(A.nc * NV, seed=1)          # B replicated on every rank
+    # Rank r owns row block r of an (N*262144) x 262144 matrix whose row
+    # blocks are independent power-law graphs; B is replicated once at setup
+    # (broadcast from rank 0), and no data crosses ranks per SpMM.
+    A = D.gen_powerlaw(NR, seed=rank)
     dA = D.DeviceCsr(A, dev)
-    Bt = torch.from_numpy(B).to(dev)
+    B = D.gen_dense(A.nc * NV, seed=1) if rank == 0 else None
+    if pg:
+        Bt = torch.from_numpy(B).to(dev) if rank == 0 else torch.empty(A.nc * NV, device=dev)
+        from daspmm.shard import broadcast_dense
+        broadcast_dense(Bt, src=0)
+    else:
+        Bt = torch.from_numpy(B).to(dev)
     Ct = torch.zeros(A.nr * NV, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
     cfg = D.default_config(alg, 0, A.nr, A.nc, A.nnz, NV) if alg != D.Alg.AUTO else None
@@ -307,6 +315,12 @@ def run_ours(args):
     if tr and tr.get("nnz") == A.nnz:
         traffic = tr.get("dram_bytes_per_launch")
 
+    # end to end through the host-buffer entry point (every rank, its block)
+    e2e = None
+    if not args.no_e2e:
+        Bh = B if B is not None else Bt.cpu().numpy()
+        e2e = run_e2e(D, A, Bh, dev, alg, min(K, args.e2e_steps), pg)
+
     line = None
     if rank == 0:
         # CPU baseline: the reference's host loop, 1 thread (it is serial), full matrix
@@ -316,10 +330,6 @@ def run_ours(args):
             cpu = {"value": round(2.0 * nnz_s * NV / (ms_cpu * 1e-3) / 1e9, 3), "unit": UNIT,
                    "cores": cores, "kind": kind,
                    "sample": f"full matrix ({nnz_s} nnz, N=128), median of 3 passes, 1 thread"}
-        # end to end through the host-buffer entry point
-        e2e = None
-        if not args.no_e2e:
-            e2e = run_e2e(D, A, B, dev, alg, min(K, args.e2e_steps))
         mixed = None if args.no_mixed else run_mixed(D, A, dA, B, dev, K, peak)
         batched = None if (args.no_batched or world > 1) else run_batched(D, dev)
         serving = None if (args.no_serving or world > 1) else run_serving(D, dev, args.serve_seconds)
@@ -542,37 +552,58 @@ def run_serving(D, dev, seconds: float = 1.0, rate: float = 20000.0):
     return out
 
 
-def run_e2e(D, A, B, dev, alg, steps):
-    """Same SpMM through daspmm_spmm_host: pinned host A, B in; C out."""
-    import numpy as np
+def run_e2e(D, A, B, dev, alg, steps, pg=None):
+    """Same SpMM through the host-buffer entry point: every step copies its
+    inputs (rowPtr, colIdx, values, B) from pinned host memory to the device,
+    runs the SpMM and copies C back to pinned host memory.  Steps alternate
+    between two streams (daspmm_spmm_host_async, each stream with its own
+    device staging and host C), so one step's C download overlaps the next
+    step's upload; timed with CUDA events around all steps (both streams
+    joined), max over ranks."""
     import torch
     L = D.lib()
     pin = lambda a: torch.from_numpy(a).pin_memory()
     rp, ci, va, Bh = pin(A.rowPtr), pin(A.colIdx), pin(A.values), pin(B)
-    Ch = torch.empty(A.nr * NV, dtype=torch.float32).pin_memory()
+    Ch = [torch.empty(A.nr * NV, dtype=torch.float32).pin_memory() for _ in range(2)]
     cfg = D.default_config(alg, 0, A.nr, A.nc, A.nnz, NV)
-    stream = torch.cuda.current_stream(dev)
-    sp = ctypes.c_void_p(stream.cuda_stream)
+    streams = [torch.cuda.Stream(dev), torch.cuda.Stream(dev)]
 
-    def once():
-        D.check(L.daspmm_spmm_host(ctypes.byref(cfg), 0, A.nr, A.nc, A.nnz, NV,
-                                   ctypes.c_void_p(rp.data_ptr()), None,
-                                   ctypes.c_void_p(ci.data_ptr()), ctypes.c_void_p(va.data_ptr()),
-                                   ctypes.c_void_p(Bh.data_ptr()), ctypes.c_void_p(Ch.data_ptr()),
-                                   0.0, sp), "spmm_host")
-    once()
-    once()
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        once()
-    dt = (time.perf_counter() - t0) / steps
+    def once(i):
+        D.check(L.daspmm_spmm_host_async(
+            ctypes.byref(cfg), 0, A.nr, A.nc, A.nnz, NV, ctypes.c_void_p(rp.data_ptr()), None,
+            ctypes.c_void_p(ci.data_ptr()), ctypes.c_void_p(va.data_ptr()),
+            ctypes.c_void_p(Bh.data_ptr()), ctypes.c_void_p(Ch[i % 2].data_ptr()), 0.0,
+            ctypes.c_void_p(streams[i % 2].cuda_stream)), "spmm_host_async")
+    for i in range(4):
+        once(i)
+    torch.cuda.synchronize(dev)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(streams[0])
+    streams[1].wait_event(e0)
+    for i in range(steps):
+        once(i)
+    streams[0].wait_stream(streams[1])
+    e1.record(streams[0])
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
     h2d = 4 * (A.nr + 1) + 8 * A.nnz + 4 * A.nc * NV
     d2h = 4 * A.nr * NV
-    return {"value": round(2.0 * A.nnz * NV / dt / 1e9, 3), "unit": UNIT,
+    flop = 2.0 * A.nnz * NV
+    if pg:
+        t = torch.tensor([ms, flop, h2d, d2h], dtype=torch.float64, device=dev)
+        mx = t.clone()
+        pg.all_reduce(mx, op=pg.ReduceOp.MAX)
+        pg.all_reduce(t, op=pg.ReduceOp.SUM)
+        ms, flop, h2d, d2h = float(mx[0]), float(t[1]), int(t[2]), int(t[3])
+    return {"value": round(flop / (ms * 1e-3) / 1e9, 3), "unit": UNIT,
             "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-            "ms_per_step": round(dt * 1e3, 4), "steps": steps,
-            "path": "daspmm_spmm_host: pinned host rowPtr/colIdx/values/B -> device, SpMM, "
-                    "C -> pinned host, stream synchronised each step"}
+            "ms_per_step": round(ms, 4), "steps": steps,
+            "path": "daspmm_spmm_host_async on two alternating streams: pinned host "
+                    "rowPtr/colIdx/values/B -> device, SpMM, C -> pinned host every step; "
+                    "CUDA events around all steps, max over ranks"}
 
 
 def main():

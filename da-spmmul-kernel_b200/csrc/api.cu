@@ -642,10 +642,10 @@ int daspmm_kernel_timer_end(float *ms_out, int n)
     return ok;
 }
 
-daspmm_status daspmm_spmm_host(const daspmm_config *cfg, int layout, int nr, int nc, int nnz,
-                               int nv, const int *rowPtr, const int *rowIdx, const int *colIdx,
-                               const float *values, const float *B, float *C, float beta,
-                               void *stream)
+static daspmm_status spmm_host_impl(const daspmm_config *cfg, int layout, int nr, int nc,
+                                    int nnz, int nv, const int *rowPtr, const int *rowIdx,
+                                    const int *colIdx, const float *values, const float *B,
+                                    float *C, float beta, void *stream, bool sync)
 {
     Resolved r;
     daspmm_status s = resolve(cfg, layout, nr, nnz, nv, nullptr, nullptr, &r);
@@ -692,8 +692,26 @@ daspmm_status daspmm_spmm_host(const daspmm_config *cfg, int layout, int nr, int
                      b_ws, st);
     if (s != DASPMM_OK) return s;
     e = cudaMemcpyAsync(C, d_C, sizeof(float) * (size_t)nr * nv, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess && sync) e = cudaStreamSynchronize(st);
     return e == cudaSuccess ? DASPMM_OK : cuda_fail(e);
+}
+
+daspmm_status daspmm_spmm_host(const daspmm_config *cfg, int layout, int nr, int nc, int nnz,
+                               int nv, const int *rowPtr, const int *rowIdx, const int *colIdx,
+                               const float *values, const float *B, float *C, float beta,
+                               void *stream)
+{
+    return spmm_host_impl(cfg, layout, nr, nc, nnz, nv, rowPtr, rowIdx, colIdx, values, B, C,
+                          beta, stream, true);
+}
+
+daspmm_status daspmm_spmm_host_async(const daspmm_config *cfg, int layout, int nr, int nc,
+                                     int nnz, int nv, const int *rowPtr, const int *rowIdx,
+                                     const int *colIdx, const float *values, const float *B,
+                                     float *C, float beta, void *stream)
+{
+    return spmm_host_impl(cfg, layout, nr, nc, nnz, nv, rowPtr, rowIdx, colIdx, values, B, C,
+                          beta, stream, false);
 }
 
 const char *daspmm_status_string(daspmm_status s)

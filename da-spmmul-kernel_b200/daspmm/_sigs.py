@@ -72,6 +72,8 @@ def apply(lib, Config):
         "daspmm_tune_clear": (None, []),
         "daspmm_spmm_host": (_I, [ctypes.POINTER(Config), _I, _I, _I, _I, _I, _VP, _VP, _VP,
                                   _VP, _VP, _VP, ctypes.c_float, _VP]),
+        "daspmm_spmm_host_async": (_I, [ctypes.POINTER(Config), _I, _I, _I, _I, _I, _VP, _VP,
+                                        _VP, _VP, _VP, _VP, ctypes.c_float, _VP]),
         "daspmm_launch_count": (ctypes.c_longlong, []),
         "daspmm_spmm_mixed": (_I, [ctypes.POINTER(Config), _I, _I, _I, _I, _I, _VP, _VP, _VP, _I,
                                    _VP, _I, _VP, _VP, ctypes.c_float, _I, _VP, ctypes.c_size_t,

@@ -362,6 +362,15 @@ daspmm_status daspmm_spmm_host(const daspmm_config *cfg, int layout, int nr, int
                                int nnz, int nv, const int *rowPtr, const int *rowIdx,
                                const int *colIdx, const float *values, const float *B,
                                float *C, float beta, void *stream);
+/* daspmm_spmm_host without the final synchronisation: the copies and the
+ * SpMM are queued on `stream` and the call returns.  A, B and C (host) must
+ * stay untouched until the stream has finished.  Calls on one stream share
+ * that stream's device staging (stream order keeps them apart); calls on
+ * different streams overlap one another's copies in both directions. */
+daspmm_status daspmm_spmm_host_async(const daspmm_config *cfg, int layout, int nr, int nc,
+                                     int nnz, int nv, const int *rowPtr, const int *rowIdx,
+                                     const int *colIdx, const float *values, const float *B,
+                                     float *C, float beta, void *stream);
 
 /* ---- No device allocation ----------------------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc
