@@ -93,17 +93,41 @@ static bool is_pow2(int x) { return x > 0 && (x & (x - 1)) == 0; }
 static bool aligned(const void *p, size_t a) { return ((uintptr_t)p % a) == 0; }
 
 // ---------------------------------------------------------------- resolve
-daspmm_status resolve(const daspmm_config *cfg, int layout, int nr, int nnz, int nv,
+daspmm_status resolve(const daspmm_config *cfg, int layout, int nr, int nc, int nnz, int nv,
                       const void *B, const void *C, Resolved *out)
 {
     if (!cfg || !out) return DASPMM_ERR_INVALID;
     if (layout != DASPMM_ROW_MAJOR && layout != DASPMM_COL_MAJOR) return DASPMM_ERR_INVALID;
     if (cfg->alg < DASPMM_ALG_CSR_SCALAR || cfg->alg > DASPMM_ALG_CSR_BALANCED)
         return DASPMM_ERR_INVALID;
-    if (nv < 1 || nr < 0 || nnz < 0) return DASPMM_ERR_INVALID;
+    if (nv < 1 || nr < 0 || nnz < 0 || nc < 0) return DASPMM_ERR_INVALID;
     Resolved r{};
     r.alg = cfg->alg;
     r.cm = layout == DASPMM_COL_MAJOR;
+    r.nr = nr;
+    r.nc = nc;
+    r.nnz = nnz;
+    if (cfg->pipe < 0 || cfg->pipe > 5) return DASPMM_ERR_INVALID;
+    if (cfg->pipe == 5 && !(r.cm && cfg->alg == DASPMM_ALG_CSR_BALANCED))
+        return DASPMM_ERR_UNSUPPORTED;
+    // Column-major balanced CSR with 4 or more columns: transpose B to
+    // row-major, run the row-major product, transpose C back (pipe 5).  A
+    // column-major gather reads one 4-byte value of a 32-byte sector per
+    // (nonzero, column); the row-major one reads whole rows of B.
+    if (r.cm && cfg->alg == DASPMM_ALG_CSR_BALANCED &&
+        (cfg->pipe == 5 || (cfg->pipe == 0 && nv >= 4 && !cfg->vec && !cfg->cf &&
+                            !cfg->lanes_col && !cfg->lanes_nnz))) {
+        r.pipe = 5;
+        r.inner_chunk = cfg->chunk;
+        r.V = 1; r.L = 1; r.S = 1; r.CF = 1;
+        r.chunk = cfg->chunk;
+        r.nchunks = 0;
+        r.snap = cfg->snap;
+        r.block = 256;
+        r.tiles = 1;
+        *out = r;
+        return DASPMM_OK;
+    }
     const bool vector = cfg->alg == DASPMM_ALG_CSR_VECTOR || cfg->alg == DASPMM_ALG_COO_VECTOR;
     // vector width
     if (r.cm) {
@@ -162,7 +186,6 @@ daspmm_status resolve(const daspmm_config *cfg, int layout, int nr, int nnz, int
     if (r.block != 128 && r.block != 256) return DASPMM_ERR_INVALID;  // __launch_bounds__(256)
     r.pipe = 1;
     r.W = 0;
-    if (cfg->pipe < 0 || cfg->pipe > 4) return DASPMM_ERR_INVALID;
     if (cfg->alg == DASPMM_ALG_CSR_BALANCED && !r.cm && cfg->pipe != 1) {
         // TMA ring: one warp per chunk, W-float tiles (16-byte accesses, one
         // vector per lane group slot); the explicit fields, if given, must agree
@@ -200,8 +223,24 @@ daspmm_status resolve(const daspmm_config *cfg, int layout, int nr, int nnz, int
     return DASPMM_OK;
 }
 
+// The row-major product inside pipe 5.
+static daspmm_status resolve_inner(const Resolved &r, int nv, const void *B, const void *C,
+                                   Resolved *in)
+{
+    daspmm_config c{};
+    c.alg = DASPMM_ALG_CSR_BALANCED;
+    c.chunk = r.inner_chunk;
+    return resolve(&c, DASPMM_ROW_MAJOR, r.nr, r.nc, r.nnz, nv, B, C, in);
+}
+
 size_t workspace_bytes(const Resolved &r, int nv)
 {
+    if (r.pipe == 5) {  // [B row-major | C row-major | the row-major product's own]
+        Resolved in;
+        if (resolve_inner(r, nv, nullptr, nullptr, &in) != DASPMM_OK) return 0;
+        return align256(sizeof(float) * (size_t)r.nc * nv) +
+               align256(sizeof(float) * (size_t)r.nr * nv) + workspace_bytes(in, nv);
+    }
     size_t b = 0;
     if (r.alg == DASPMM_ALG_CSR_BALANCED) {
         b += align256(sizeof(int2) * ((size_t)r.nchunks + 1));
@@ -308,6 +347,17 @@ static daspmm_status dispatch(const Resolved &r, KArgs &a, dim3 grid, dim3 fix_g
     return DASPMM_ERR_UNSUPPORTED;
 }
 
+// dst (Cn x R, row-major) = transpose of src (R x Cn, row-major) + beta * dst.
+static void launch_transpose(const float *src, long long R, long long Cn, float *dst, float beta,
+                             cudaStream_t st)
+{
+    const long long tiles = ((R + 31) / 32) * ((Cn + 31) / 32);
+    const unsigned g = (unsigned)std::max<long long>(
+        1, std::min<long long>(tiles, (long long)device_sms() * 16));
+    k_transpose<<<g, dim3(32, 8), 0, st>>>(src, R, Cn, dst, beta);
+    count_launches(1);
+}
+
 static unsigned grid_x(long long units, int G, int block)
 {
     const long long gpb = (long long)(block / 32) * (32 / G);
@@ -331,6 +381,23 @@ daspmm_status run_resolved(const Resolved &r, int layout, int nr, int nc, int nn
     if (nc <= 0 && nnz > 0) return DASPMM_ERR_INVALID;
     const size_t need = workspace_bytes(r, nv);
     if (need > ws_bytes || (need && !ws)) return DASPMM_ERR_WORKSPACE;
+
+    if (r.pipe == 5) {
+        float *Brm = (float *)ws;
+        float *Crm = (float *)((char *)ws + align256(sizeof(float) * (size_t)nc * nv));
+        char *iws = (char *)Crm + align256(sizeof(float) * (size_t)nr * nv);
+        Resolved in;
+        daspmm_status s = resolve_inner(r, nv, Brm, Crm, &in);
+        if (s != DASPMM_OK) return s;
+        // B column-major = an nv x nc row-major array; its transpose is row-major B
+        launch_transpose(B, nv, nc, Brm, 0.0f, st);
+        s = run_resolved(in, DASPMM_ROW_MAJOR, nr, nc, nnz, nv, rowPtr, rowIdx, colIdx, values,
+                         Brm, Crm, 0.0f, iws, workspace_bytes(in, nv), st);
+        if (s != DASPMM_OK) return s;
+        launch_transpose(Crm, nr, nv, C, beta, st);  // C = transpose + beta * C
+        const cudaError_t e = cudaGetLastError();
+        return e == cudaSuccess ? DASPMM_OK : cuda_fail(e);
+    }
 
     KArgs a{};
     a.nr = nr; a.nc = nc; a.nnz = nnz; a.nv = nv;
@@ -448,16 +515,17 @@ daspmm_status daspmm_default_config(int alg, int layout, int nr, int nc, int nnz
     daspmm_config c{};
     c.alg = alg;
     Resolved r;
-    daspmm_status s = resolve(&c, layout, nr, nnz, nv, nullptr, nullptr, &r);
+    daspmm_status s = resolve(&c, layout, nr, nc, nnz, nv, nullptr, nullptr, &r);
     if (s != DASPMM_OK) return s;
     *out = to_config(r);
     return DASPMM_OK;
 }
 
-size_t daspmm_workspace_bytes(const daspmm_config *cfg, int layout, int nr, int nnz, int nv)
+size_t daspmm_workspace_bytes(const daspmm_config *cfg, int layout, int nr, int nc, int nnz,
+                              int nv)
 {
     Resolved r;
-    if (resolve(cfg, layout, nr, nnz, nv, nullptr, nullptr, &r) != DASPMM_OK) return 0;
+    if (resolve(cfg, layout, nr, nc, nnz, nv, nullptr, nullptr, &r) != DASPMM_OK) return 0;
     return workspace_bytes(r, nv);
 }
 
@@ -468,7 +536,7 @@ daspmm_status daspmm_spmm_ex(const daspmm_config *cfg, int layout, int nr, int n
                              void *stream)
 {
     Resolved r;
-    daspmm_status s = resolve(cfg, layout, nr, nnz, nv, B, C, &r);
+    daspmm_status s = resolve(cfg, layout, nr, nc, nnz, nv, B, C, &r);
     if (s != DASPMM_OK) return s;
     cudaStream_t st = (cudaStream_t)stream;
     if (!workspace) {
@@ -648,7 +716,7 @@ static daspmm_status spmm_host_impl(const daspmm_config *cfg, int layout, int nr
                                     float *C, float beta, void *stream, bool sync)
 {
     Resolved r;
-    daspmm_status s = resolve(cfg, layout, nr, nnz, nv, nullptr, nullptr, &r);
+    daspmm_status s = resolve(cfg, layout, nr, nc, nnz, nv, nullptr, nullptr, &r);
     if (s != DASPMM_OK) return s;
     if (nr == 0) return DASPMM_OK;
     if (nr < 0 || nc < 0 || nnz < 0 || !B || !C) return DASPMM_ERR_INVALID;

@@ -15,11 +15,14 @@ namespace daspmm {
 struct Resolved {
     int alg;
     bool cm;
+    int nr, nc, nnz;  // the problem it was resolved for
     int V, L, S, CF;
     int chunk, snap, nchunks;
     int block, tiles;
-    int pipe;  // balanced CSR: 1 register gather, 2 TMA ring
+    int pipe;  // balanced CSR: 1 register gather, 2 TMA ring, 3 cp.async ring, 4 lean
+               // gather, 5 column-major through a row-major product (transposes)
     int W;     // TMA ring: tile width in floats (32, 64, 128)
+    int inner_chunk;  // pipe 5: the caller's chunk for the row-major product
 };
 
 // SMs of the current device (148 when no device is visible).
@@ -45,7 +48,7 @@ inline daspmm_config to_config(const Resolved &r)
 extern thread_local int g_last_cuda;
 daspmm_status cuda_fail(cudaError_t e);
 
-daspmm_status resolve(const daspmm_config *cfg, int layout, int nr, int nnz, int nv,
+daspmm_status resolve(const daspmm_config *cfg, int layout, int nr, int nc, int nnz, int nv,
                       const void *B, const void *C, Resolved *out);
 size_t workspace_bytes(const Resolved &r, int nv);
 daspmm_status run_resolved(const Resolved &r, int layout, int nr, int nc, int nnz, int nv,

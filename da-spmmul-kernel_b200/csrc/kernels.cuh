@@ -762,6 +762,34 @@ __global__ void __launch_bounds__(256) k_fix_bal(const KArgs a)
 
 // C = beta * C over an nr x nv block (used before COO accumulation when
 // beta != 1, since COO never visits rows without nonzeros).
+// dst (Cn x R) = transpose of src (R x Cn) + beta * dst, both row-major: 32 x 32
+// tiles through shared memory (reads and writes are 128-byte rows), the grid
+// striding over tiles.  beta == 0 never reads dst.
+static __global__ void __launch_bounds__(256) k_transpose(const float *__restrict__ src,
+                                                          long long R, long long Cn,
+                                                          float *__restrict__ dst, float beta)
+{
+    __shared__ float tile[32][33];
+    const long long tx = (Cn + 31) / 32, ty = (R + 31) / 32;
+    for (long long t = blockIdx.x; t < tx * ty; t += gridDim.x) {
+        const long long r0 = (t / tx) * 32, c0 = (t % tx) * 32;
+        for (int i = threadIdx.y; i < 32; i += 8) {
+            const long long r = r0 + i, c = c0 + threadIdx.x;
+            if (r < R && c < Cn) tile[i][threadIdx.x] = __ldg(src + r * Cn + c);
+        }
+        __syncthreads();
+        for (int i = threadIdx.y; i < 32; i += 8) {
+            const long long c = c0 + i, r = r0 + threadIdx.x;  // dst row c, column r
+            if (c < Cn && r < R) {
+                float *d = dst + c * R + r;
+                const float v = tile[threadIdx.x][i];
+                *d = beta == 0.0f ? v : fmaf(beta, *d, v);
+            }
+        }
+        __syncthreads();
+    }
+}
+
 static __global__ void k_scale(float *C, size_t n, float beta)
 {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;

@@ -119,7 +119,7 @@ daspmm_status daspmm_spmm_mixed(const daspmm_config *cfg_in, int layout, int nr,
     if (cfg.pipe && cfg.pipe != 4) return DASPMM_ERR_UNSUPPORTED;
     cfg.pipe = 4;
     Resolved r;
-    daspmm_status s = resolve(&cfg, layout, nr, nnz, nv, nullptr, C, &r);
+    daspmm_status s = resolve(&cfg, layout, nr, nc, nnz, nv, nullptr, C, &r);
     if (s != DASPMM_OK) return s;
     if (r.pipe != 4) return DASPMM_ERR_UNSUPPORTED;  // needs nv % 32 == 0
     const int VL = r.W / 32;

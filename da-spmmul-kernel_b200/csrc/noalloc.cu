@@ -53,8 +53,11 @@ extern "C" daspmm_status daspmm_spmm_noalloc(int layout, int nr, int nc, int nnz
 {
     daspmm_config cfg{};
     cfg.alg = DASPMM_ALG_CSR_BALANCED;
+    // column-major: the direct gather (the transposing path would need
+    // scratch for copies of B and C)
+    if (layout == DASPMM_COL_MAJOR) cfg.pipe = 1;
     daspmm::Resolved r;
-    daspmm_status s = daspmm::resolve(&cfg, layout, nr, nnz, nv, B, C, &r);
+    daspmm_status s = daspmm::resolve(&cfg, layout, nr, nc, nnz, nv, B, C, &r);
     if (s != DASPMM_OK) return s;
     // Too large for the fixed scratch: refuse before touching the device.
     if (daspmm::workspace_bytes(r, nv) > (size_t)DASPMM_NOALLOC_MAX_BYTES)

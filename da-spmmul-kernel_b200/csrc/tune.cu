@@ -134,6 +134,10 @@ std::vector<daspmm_config> candidates(int layout, int nv, bool have_coo)
         if (layout == DASPMM_COL_MAJOR)
             for (int cf : {2, 4, 8}) add(DASPMM_ALG_CSR_SCALAR, 0, 0, 0, cf);
     }
+    if (layout == DASPMM_COL_MAJOR && nv >= 4) {  // through a row-major product
+        add(DASPMM_ALG_CSR_BALANCED, 5);
+        add(DASPMM_ALG_CSR_BALANCED, 5, 256);
+    }
     return v;
 }
 
@@ -187,7 +191,7 @@ daspmm_status tuned_config(int layout, int nr, int nc, int nnz, int nv, daspmm_c
     c.alg = (layout == DASPMM_ROW_MAJOR && nv >= 32) ? DASPMM_ALG_CSR_BALANCED
                                                       : DASPMM_ALG_CSR_SCALAR;
     Resolved r;
-    daspmm_status s = resolve(&c, layout, nr, nnz, nv, nullptr, nullptr, &r);
+    daspmm_status s = resolve(&c, layout, nr, nc, nnz, nv, nullptr, nullptr, &r);
     if (s != DASPMM_OK) return s;
     *out = to_config(r);
     return DASPMM_OK;
@@ -223,7 +227,7 @@ daspmm_status daspmm_autotune(int layout, int nr, int nc, int nnz, int nv, const
     for (const daspmm_config &c0 : candidates(layout, nv, rowIdx != nullptr)) {
         // resolve to the concrete point (so the cache holds explicit values)
         Resolved r;
-        if (resolve(&c0, layout, nr, nnz, nv, B, C, &r) != DASPMM_OK) continue;
+        if (resolve(&c0, layout, nr, nc, nnz, nv, B, C, &r) != DASPMM_OK) continue;
         const daspmm_config c = to_config(r);
         bool ok = false;
         const float us = time_config(c, layout, nr, nc, nnz, nv, rowPtr, rowIdx, colIdx, values,

@@ -90,7 +90,7 @@ def _lib():
             "daspmm_spmm_ex": (_I, [ctypes.POINTER(Config), _I, _I, _I, _I, _I, _VP, _VP, _VP,
                                     _VP, _VP, _VP, ctypes.c_float, _VP, ctypes.c_size_t, _VP]),
             "daspmm_workspace_bytes": (ctypes.c_size_t,
-                                       [ctypes.POINTER(Config), _I, _I, _I, _I]),
+                                       [ctypes.POINTER(Config), _I, _I, _I, _I, _I]),
             "daspmm_default_config": (_I, [_I, _I, _I, _I, _I, _I, ctypes.POINTER(Config)]),
             "daspmm_compat_spmm": (_I, [_I, _I, _I, _I, _I, _I, _VP, _VP, _VP, _VP, _VP, _VP]),
             "daspmm_num_chunks": (_I, [_I, _I]),
@@ -223,8 +223,8 @@ def num_chunks(nnz: int, chunk: int) -> int:
     return _lib().daspmm_num_chunks(nnz, chunk)
 
 
-def workspace_bytes(cfg: Config, layout: int, nr: int, nnz: int, nv: int) -> int:
-    return _lib().daspmm_workspace_bytes(ctypes.byref(cfg), int(layout), nr, nnz, nv)
+def workspace_bytes(cfg: Config, layout: int, nr: int, nc: int, nnz: int, nv: int) -> int:
+    return _lib().daspmm_workspace_bytes(ctypes.byref(cfg), int(layout), nr, nc, nnz, nv)
 
 
 # ---------------------------------------------------------------- device side
@@ -430,6 +430,28 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------- Matrix Market
+def mtx_info(path: str) -> dict:
+    from ._sigs import MtxHeader
+    h = MtxHeader()
+    check(_lib().daspmm_mtx_info(os.fsencode(path), ctypes.byref(h)), f"mtx_info {path}")
+    return {n: getattr(h, n) for n, _ in h._fields_}
+
+
+def read_mtx(path: str, keep_diagonal: bool = False) -> Csr:
+    """A Matrix Market coordinate file as a sorted CSR (daspmm_mtx_read)."""
+    h = mtx_info(path)
+    cap = int(h["nnz_max"])
+    rp = np.zeros(h["nr"] + 1, np.int32)
+    ci = np.zeros(max(1, cap), np.int32)
+    va = np.zeros(max(1, cap), np.float32)
+    n = ctypes.c_int()
+    check(_lib().daspmm_mtx_read(os.fsencode(path), 1 if keep_diagonal else 0, cap,
+                                 rp.ctypes.data, None, ci.ctypes.data, va.ctypes.data,
+                                 ctypes.byref(n)), f"mtx_read {path}")
+    return Csr(h["nr"], h["nc"], rp, ci[: n.value].copy(), va[: n.value].copy())
 
 
 # ---------------------------------------------------------------- validation

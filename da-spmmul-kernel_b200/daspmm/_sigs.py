@@ -51,6 +51,12 @@ class ServeStats(ctypes.Structure):
                [(n, _I) for n in ("max_group", "inflight_groups", "matrices", "error")]
 
 
+class MtxHeader(ctypes.Structure):
+    """daspmm_mtx_header (include/daspmm.h)."""
+    _fields_ = [("nr", _I), ("nc", _I), ("entries", _LL), ("field", _I), ("symmetry", _I),
+                ("nnz_max", _LL)]
+
+
 def apply(lib, Config):
     sig = {
         "daspmm_batch_create": (_I, [ctypes.POINTER(Instance), _I, ctypes.POINTER(Config),
@@ -81,6 +87,9 @@ def apply(lib, Config):
         "daspmm_quantize": (_I, [_I, ctypes.c_size_t, _VP, _VP, _VP, _I, _VP]),
         "daspmm_e4m3_scales": (_I, [_I, _I, _VP, _VP, _VP]),
         "daspmm_device_error": (_I, []),
+        "daspmm_mtx_info": (_I, [ctypes.c_char_p, ctypes.POINTER(MtxHeader)]),
+        "daspmm_mtx_read": (_I, [ctypes.c_char_p, _I, _LL, _VP, _VP, _VP, _VP,
+                                 ctypes.POINTER(_I)]),
         "daspmm_csr_check": (_I, [_I, _I, _I, _VP, _VP, _I, ctypes.POINTER(_I), _VP]),
         "daspmm_server_create": (_I, [ctypes.POINTER(ServerConfig), ctypes.POINTER(_VP)]),
         "daspmm_server_add_matrix": (_I, [_VP, _I, _I, _I, _VP, _VP, _VP, ctypes.POINTER(_I)]),

@@ -76,7 +76,10 @@ typedef struct daspmm_config {
     int pipe;       /* balanced CSR, row-major: 1 = register gather; a shared-memory
                        ring fed by 2 = TMA bulk copies, 3 = 16-byte cp.async;
                        4 = lean register gather at high occupancy (2..4 need
-                       nv % 32 == 0 and 16-byte aligned B and C);
+                       nv % 32 == 0 and 16-byte aligned B and C).  Column-major:
+                       1 = direct gather, 5 = B transposed to row-major, the
+                       row-major product, C transposed back (the default from
+                       nv >= 4; A read once for all columns).
                        0 = the library's choice */
 } daspmm_config;
 
@@ -104,8 +107,9 @@ daspmm_status daspmm_spmm_ex(const daspmm_config *cfg, int layout, int nr, int n
                              float *C, float beta, void *workspace, size_t ws_bytes,
                              void *stream);
 
-/* Workspace bytes daspmm_spmm_ex needs for this configuration and shape. */
-size_t daspmm_workspace_bytes(const daspmm_config *cfg, int layout, int nr, int nnz,
+/* Workspace bytes daspmm_spmm_ex needs for this configuration and shape
+ * (pipe 5 holds row-major copies of B and C, so nc matters). */
+size_t daspmm_workspace_bytes(const daspmm_config *cfg, int layout, int nr, int nc, int nnz,
                               int nv);
 
 /* Fill *out with the configuration the library would use for this shape
@@ -252,6 +256,36 @@ daspmm_status daspmm_batch_destroy(daspmm_batch b);
 daspmm_status daspmm_batch_tune(const daspmm_instance *inst, int n, const int *chunks,
                                 int nchunks, int reps, int *best_chunk, float *best_us,
                                 void *stream);
+
+/* ---- Matrix Market input ---------------------------------------------------
+ * Coordinate files (real, integer or pattern values; general, symmetric,
+ * skew-symmetric or hermitian) to CSR sorted by (row, col).  Replaces
+ * readMtx (util/spmatrix.hpp:286-333) with makeSymmetric
+ * (spmatrix.hpp:219-284): a symmetric file is mirrored and loses its diagonal
+ * and repeated (row, col) pairs, as in the reference, but every value stays
+ * with its own (row, col) (the reference compacts rows and columns only, so
+ * its values after the first dropped entry are misplaced).  Skew-symmetric
+ * and hermitian files are read as stored (the reference does not mirror
+ * them either); pattern entries have value 1; repeated pairs of a general
+ * file are kept, in file order. */
+#define DASPMM_MTX_KEEP_DIAGONAL 1   /* symmetric files: keep diagonal entries */
+
+typedef struct daspmm_mtx_header {
+    int nr, nc;
+    long long entries;   /* entries stored in the file */
+    int field;           /* 0 real, 1 integer, 2 pattern, 3 complex */
+    int symmetry;        /* 0 general, 1 symmetric, 2 skew-symmetric, 3 hermitian */
+    long long nnz_max;   /* capacity that daspmm_mtx_read needs at most */
+} daspmm_mtx_header;
+
+daspmm_status daspmm_mtx_info(const char *path, daspmm_mtx_header *out);
+/* Host arrays: rowPtr[nr+1]; rowIdx (may be NULL: the COO row of each
+ * nonzero), colIdx and values of capacity `cap` (>= the nonzeros produced,
+ * DASPMM_ERR_WORKSPACE otherwise).  DASPMM_ERR_BAD_MATRIX for a malformed
+ * file (bad banner or size line, an index out of range, fewer entries than
+ * the size line says); DASPMM_ERR_UNSUPPORTED for complex or dense files. */
+daspmm_status daspmm_mtx_read(const char *path, int flags, long long cap, int *rowPtr,
+                              int *rowIdx, int *colIdx, float *values, int *nnz_out);
 
 /* ---- CSR validation -------------------------------------------------------
  * Checks a device CSR matrix: rowPtr[0] == 0, rowPtr[nr] == nnz, rowPtr

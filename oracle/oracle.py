@@ -236,3 +236,40 @@ def rel_err(c, c64, absc) -> float:
     if bad.any():
         return float("inf")
     return float((d / scale).max()) if d.size else 0.0
+
+
+def read_mtx(path: str, keep_diagonal: bool = False):
+    """readMtx<float> (util/spmatrix.hpp:286-333) restated for small files,
+    with makeSymmetric's value alignment fixed: returns (nr, nc, rows, cols,
+    vals) sorted by (row, col, position in the file).  A symmetric file is
+    mirrored (spmatrix.hpp:225-232) and loses diagonal entries and repeated
+    (row, col) pairs (:244-263); pattern entries have value 1 (:166-180)."""
+    with open(path) as f:
+        lines = f.read().split("\n")
+    banner = lines[0].lower().split()
+    field, sym = banner[3], banner[4]
+    i = 1
+    while not lines[i].strip() or lines[i].lstrip().startswith("%"):
+        i += 1
+    nr, nc, nz = (int(x) for x in lines[i].split()[:3])
+    ent = []
+    for k, line in enumerate(lines[i + 1: i + 1 + nz]):
+        t = line.split()
+        v = 1.0 if field == "pattern" else float(np.float32(float(t[2])))
+        ent.append((int(t[0]) - 1, int(t[1]) - 1, k, v))
+    if sym == "symmetric":
+        ent += [(c, r, nz + k, v) for (r, c, k, v) in ent if r != c]
+    ent.sort(key=lambda e: (e[0], e[1], e[2]))
+    if sym == "symmetric":
+        kept = []
+        for e in ent:
+            if e[0] == e[1] and not keep_diagonal:
+                continue
+            if kept and kept[-1][0] == e[0] and kept[-1][1] == e[1]:
+                continue
+            kept.append(e)
+        ent = kept
+    rows = np.array([e[0] for e in ent], np.int32)
+    cols = np.array([e[1] for e in ent], np.int32)
+    vals = np.array([e[3] for e in ent], np.float32)
+    return nr, nc, rows, cols, vals

@@ -148,4 +148,26 @@ float ref_cusparse_bench(int format, int layout, int nr, int nc, int nnz, int nv
                           (cusparseSpMMAlg_t)alg, reps, warmup);
 }
 
+/* readMtx<float> (util/spmatrix.hpp:286-333), makeSymmetric included, on a
+ * Matrix Market file: fills up to `cap` (row, col, value) triples in the
+ * reference's output order and returns how many it produced (-1 when `cap`
+ * is too small).  The reference exits the process on a missing file or a bad
+ * banner, so only well-formed files may be passed. */
+int ref_read_mtx(const char *path, int *nr, int *nc, int cap, int *rows, int *cols,
+                 float *vals)
+{
+    IdxArray ri, ci;
+    ValArray va;
+    int nvals = 0;
+    readMtx<float>(path, ri, ci, va, *nr, *nc, nvals);
+    const int n = (int)ri.size();
+    if (n > cap) return -1;
+    for (int i = 0; i < n; ++i) {
+        rows[i] = ri[i];
+        cols[i] = ci[i];
+        vals[i] = i < (int)va.size() ? va[i] : 0.0f;
+    }
+    return n;
+}
+
 } /* extern "C" */

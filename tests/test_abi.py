@@ -49,10 +49,13 @@ def test_default_configs():
     # the TMA ring sizes one wave of chunks over 148 SMs x 12 warps (no GPU here: 148)
     r = D.Config(alg=4, pipe=2)
     c = D.default_config(D.Alg.CSR_BALANCED, D.Layout.ROW_MAJOR, 262144, 262144, 1_227_000, 128)
-    assert D.workspace_bytes(r, 0, 262144, 1_227_000, 128) > 0
+    assert D.workspace_bytes(r, 0, 262144, 262144, 1_227_000, 128) > 0
     c = D.default_config(D.Alg.CSR_BALANCED, D.Layout.ROW_MAJOR, 1000, 1000, 9000, 30)
     assert c.pipe == 1 and c.chunk == 64           # nv % 32 != 0: register gather (V=2, L=16)
     c = D.default_config(D.Alg.CSR_BALANCED, D.Layout.COL_MAJOR, 1000, 1000, 9000, 64)
+    assert c.pipe == 5                             # column-major through row-major
+    assert D.workspace_bytes(c, 1, 1000, 800, 9000, 64) >= (1000 + 800) * 64 * 4
+    c = D.default_config(D.Alg.CSR_BALANCED, D.Layout.COL_MAJOR, 1000, 1000, 9000, 2)
     assert c.pipe == 1
     c = D.default_config(D.Alg.CSR_VECTOR, D.Layout.ROW_MAJOR, 100, 100, 1000, 1)
     assert (c.vec, c.lanes_col, c.lanes_nnz) == (1, 1, 32)
@@ -85,8 +88,9 @@ def test_invalid_arguments_rejected_before_any_device_work():
 def test_workspace_bytes():
     cfg = D.default_config(D.Alg.CSR_BALANCED, 0, 1000, 1000, 10000, 64)
     nch = D.num_chunks(10000, cfg.chunk)
-    assert D.workspace_bytes(cfg, 0, 1000, 10000, 64) >= nch * 2 * 64 * 4 + (nch + 1) * 8
-    assert D.workspace_bytes(D.default_config(0, 0, 1000, 1000, 10000, 64), 0, 1000, 10000, 64) == 0
+    assert D.workspace_bytes(cfg, 0, 1000, 1000, 10000, 64) >= nch * 2 * 64 * 4 + (nch + 1) * 8
+    assert D.workspace_bytes(D.default_config(0, 0, 1000, 1000, 10000, 64), 0, 1000, 1000, 10000,
+                             64) == 0
     assert D.num_chunks(0, 128) == 1 and D.num_chunks(129, 128) == 2 and D.num_chunks(5, 0) == -1
 
 

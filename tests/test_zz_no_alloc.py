@@ -84,7 +84,7 @@ def test_full_size_power_law_fits_and_matches(cuda):
     dA = D.DeviceCsr(A)
     B = D.gen_dense(A.nc * 128, seed=1)
     cfg = D.default_config(D.Alg.CSR_BALANCED, 0, A.nr, A.nc, A.nnz, 128)
-    assert D.workspace_bytes(cfg, 0, A.nr, A.nnz, 128) <= (16 << 20)
+    assert D.workspace_bytes(cfg, 0, A.nr, A.nc, A.nnz, 128) <= (16 << 20)
     for _ in range(2):
         Cn, Ce = _both(A, dA, 0, 128, B)
         ok, bad = O.check_result(0, 0, A.nr, 128, Ce, Cn, O.REF_ABS_TOL)
@@ -98,7 +98,7 @@ def test_too_large_is_refused_before_device_work(cuda):
     nnz = 2_200_000
     nv = 4096
     cfg = D.default_config(D.Alg.CSR_BALANCED, 0, nr, nr, nnz, nv)
-    assert D.workspace_bytes(cfg, 0, nr, nnz, nv) > (16 << 20)
+    assert D.workspace_bytes(cfg, 0, nr, nr, nnz, nv) > (16 << 20)
     dummy = torch.zeros(4, dtype=torch.float32, device="cuda")
     st = _noalloc()(0, nr, nr, nnz, nv, _p(dummy), _p(dummy), _p(dummy), _p(dummy), _p(dummy),
                     0.0, None)
