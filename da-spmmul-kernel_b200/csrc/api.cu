@@ -245,6 +245,8 @@ size_t workspace_bytes(const Resolved &r, int nv)
     if (r.alg == DASPMM_ALG_CSR_BALANCED) {
         b += align256(sizeof(int2) * ((size_t)r.nchunks + 1));
         b += align256(sizeof(int) * (size_t)r.nchunks * r.tiles);  // split-row arrival counters
+        b += align256(sizeof(unsigned int) * (size_t)r.tiles);     // chunk queue heads
+        b += align256(sizeof(int) * ((size_t)r.nchunks + 1));      // chunks left to the walk
     }
     if (r.alg >= DASPMM_ALG_COO_SCALAR) b += align256(sizeof(float) * 2 * (size_t)r.nchunks * nv);
     return b;
@@ -277,12 +279,7 @@ static void launch_ring(const Resolved &r, const KArgs &a, cudaStream_t st)
 template <int W>
 static void launch_lean_w(const Resolved &r, const KArgs &a, cudaStream_t st)
 {
-    // at most the CTAs that fit at once (grid-stride over chunks beyond that):
-    // no partial second wave
-    const long long resident = (long long)device_sms() * DASPMM_LEAN_MINB;
-    const unsigned gx = (unsigned)std::max<long long>(
-        1, std::min<long long>(((long long)a.nchunks + 7) / 8, resident));
-    k_bal_lean<W, DASPMM_LEAN_U><<<dim3(gx, r.tiles), 256, 0, st>>>(a);
+    launch_lean<W, float, float, false>(r, a, st);
 }
 
 static void launch_tma(const Resolved &r, const KArgs &a, cudaStream_t st)
@@ -422,15 +419,8 @@ daspmm_status run_resolved(const Resolved &r, int layout, int nr, int nc, int nn
         }
         a.slots = (float *)ws;
     } else if (r.alg == DASPMM_ALG_CSR_BALANCED) {
-        int2 *meta = (int2 *)ws;
-        char *p = (char *)ws + align256(sizeof(int2) * ((size_t)r.nchunks + 1));
-        a.meta = meta;
-        a.cnt = (int *)p;
-        a.slots = (float *)(p + align256(sizeof(int) * (size_t)r.nchunks * r.tiles));
-        const unsigned pg = (unsigned)std::max(1, (nr + 255) / 256);
-        k_partition<<<pg, 256, 0, st>>>(nr, nnz, rowPtr, r.chunk, r.snap, r.nchunks, meta,
-                                         a.cnt, r.tiles);
-        count_launches(1);
+        carve_balanced(r, ws, &a);
+        launch_partition(r, nr, nnz, rowPtr, a, st);
     }
     const long long units =
         (r.alg == DASPMM_ALG_CSR_SCALAR || r.alg == DASPMM_ALG_CSR_VECTOR) ? nr : r.nchunks;
@@ -440,6 +430,30 @@ daspmm_status run_resolved(const Resolved &r, int layout, int nr, int nc, int nn
     if (s != DASPMM_OK) return s;
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? DASPMM_OK : cuda_fail(e);
+}
+
+void carve_balanced(const Resolved &r, void *ws, KArgs *a)
+{
+    char *p = (char *)ws;
+    a->meta = (const int2 *)p;
+    p += align256(sizeof(int2) * ((size_t)r.nchunks + 1));
+    a->cnt = (int *)p;
+    p += align256(sizeof(int) * (size_t)r.nchunks * r.tiles);
+    a->head = (unsigned int *)p;
+    p += align256(sizeof(unsigned int) * (size_t)r.tiles);
+    a->list = (int *)p;
+    p += align256(sizeof(int) * ((size_t)r.nchunks + 1));
+    a->slots = (float *)p;
+}
+
+void launch_partition(const Resolved &r, int nr, int nnz, const int *rowPtr, const KArgs &a,
+                      cudaStream_t st)
+{
+    const unsigned pg = (unsigned)std::max(1, (nr + 255) / 256);
+    k_partition<<<pg, 256, 0, st>>>(nr, nnz, rowPtr, r.chunk, r.snap, r.nchunks,
+                                     const_cast<int2 *>(a.meta), a.cnt, r.tiles, a.head,
+                                     a.list);
+    count_launches(1);
 }
 
 // ---------------------------------------------------------------- workspace
@@ -595,7 +609,8 @@ daspmm_status daspmm_partition(int nr, int nnz, const int *rowPtr, int chunk, in
     const int nch = daspmm_num_chunks(nnz, chunk);
     const unsigned pg = (unsigned)std::max(1, (nr + 255) / 256);
     k_partition<<<pg, 256, 0, (cudaStream_t)stream>>>(nr, nnz, rowPtr, chunk, std::min(snap, chunk),
-                                                      nch, (int2 *)meta, nullptr, 1);
+                                                      nch, (int2 *)meta, nullptr, 1, nullptr,
+                                                      nullptr);
     count_launches(1);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? DASPMM_OK : cuda_fail(e);

@@ -28,6 +28,7 @@
 #include <cuda_fp16.h>
 #include <cuda_fp8.h>
 
+#include "internal.h"
 #include "kernels.cuh"
 #include "tma.cuh"
 
@@ -112,9 +113,16 @@ __global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_lean(const KArgs 
 #pragma unroll
     for (int e = 0; e < VL; ++e) sc[e] = SCALED ? __ldg(a.bscale + tb + e) : 1.0f;
 
-    for (long long cl = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; cl < a.nchunks;
-         cl += nwarps) {
-        const int c = (int)cl;
+    // Queue mode: chunks are handed out dynamically -- each warp starts with
+    // chunk = its index, then takes the next unclaimed one from the column
+    // tile's queue head (zeroed by k_partition), so warps that draw short
+    // chunks take more and no wave of chunks is left half-used.  List mode:
+    // the chunks k_bal_fast left over (a.list), strided over the warps.
+    const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long limit = a.list_mode ? (long long)a.list[0] : (long long)a.nchunks;
+    long long cl = wid;
+    while (cl < limit) {
+        const int c = a.list_mode ? a.list[1 + cl] : (int)cl;
         const int2 m0 = a.meta[c], m1 = a.meta[c + 1];
         const int k0 = m0.x, k1 = m1.x, s1 = m1.y;
         int r = m0.y;
@@ -229,6 +237,165 @@ __global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_lean(const KArgs 
         // the last piece of a row adds them all)
         if (head_piece) piece_arrive<VL>(a, head_row, tb);
         if (tail_piece) piece_arrive<VL>(a, s1, tb);
+        if (a.list_mode) {
+            cl += nwarps;
+        } else {
+            unsigned int nx = 0;
+            if (lane == 0) nx = atomicAdd(a.head + blockIdx.y, 1u);
+            cl = nwarps + (long long)__shfl_sync(kFull, nx, 0);
+        }
+    }
+}
+
+// Balanced-CSR SpMM, beta == 0, for chunks without empty rows: the ends of
+// the rows finishing in a window of 32 nonzeros come as one bitmask (lane l
+// looks at the end of row r + l; with no empty row the 32 lanes cover every
+// row that can end in the window), so the window is summed straight through
+// -- no per-nonzero test against a row end -- and a row is stored at its bit.
+// A chunk holding an empty row is left untouched and listed in a.list for
+// k_bal_lean (list mode), launched after this kernel.  Same chunks, carries
+// and split-row combine as k_bal_lean, so results are identical to it.
+template <int W, int U, typename TV = float, typename TB = float>
+__global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_fast(const KArgs a)
+{
+    constexpr int VL = W / 32;
+    constexpr bool SCALED = std::is_same<TB, fp8>::value;
+    const int lane = threadIdx.x & 31;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const int tb = blockIdx.y * W + lane * VL;
+    const TB *Bl = reinterpret_cast<const TB *>(a.B) + tb;
+    const TV *Av = reinterpret_cast<const TV *>(a.vals);
+    const uint64_t pol_once = policy_evict_first();
+    float sc[VL];
+#pragma unroll
+    for (int e = 0; e < VL; ++e) sc[e] = SCALED ? __ldg(a.bscale + tb + e) : 1.0f;
+
+    long long cl = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    while (cl < a.nchunks) {
+        const int c = (int)cl;
+        const int2 m0 = a.meta[c], m1 = a.meta[c + 1];
+        const int k0 = m0.x, k1 = m1.x, s1 = m1.y;
+        int r = m0.y;
+        const int rstart = __ldg(a.rowPtr + r);
+        // ends of rows r .. r+31; any empty row among [r, s1) hands the chunk on
+        int E = __ldg(a.rowPtr + min(r + 1 + lane, a.nr));
+        bool empty_row;
+        {
+            int prev = __shfl_up_sync(kFull, E, 1);
+            if (lane == 0) prev = rstart;
+            empty_row = __any_sync(kFull, r + lane < s1 && E == prev);
+            int last = __shfl_sync(kFull, E, 31);
+            for (int rb = r + 32; !empty_row && rb < s1; rb += 32) {
+                const int e2 = __ldg(a.rowPtr + min(rb + 1 + lane, a.nr));
+                int p2 = __shfl_up_sync(kFull, e2, 1);
+                if (lane == 0) p2 = last;
+                empty_row = __any_sync(kFull, rb + lane < s1 && e2 == p2);
+                last = __shfl_sync(kFull, e2, 31);
+            }
+        }
+        if (empty_row) {
+            if (blockIdx.y == 0 && lane == 0) a.list[1 + atomicAdd(a.list, 1)] = c;
+        } else {
+            bool cont = k0 > rstart;
+            const bool head_piece = cont;
+            float acc[VL];
+#pragma unroll
+            for (int e = 0; e < VL; ++e) acc[e] = 0.0f;
+            auto load_win = [&](int wb, int &col, float &val) {
+                const bool ok = wb + lane < k1;
+                col = ok ? ld_hint_s32(a.colIdx + wb + lane, pol_once) : 0;
+                val = ok ? ld_val<TV>(Av + wb + lane, pol_once) : 0.0f;
+            };
+            int ccur, cnext;
+            float vcur, vnext;
+            load_win(k0, ccur, vcur);
+            for (int wb = k0; wb < k1; wb += 32) {
+                load_win(wb + 32, cnext, vnext);
+                const int cnt = min(32, k1 - wb);
+                const int pos = E - 1 - wb;
+                const bool in = r + 1 + lane <= a.nr && pos >= 0 && pos < cnt;
+                const unsigned ends = __reduce_or_sync(kFull, in ? (1u << pos) : 0u);
+                // the next window's row ends load while this one is summed
+                E = __ldg(a.rowPtr + min(r + __popc(ends) + 1 + lane, a.nr));
+                float *cdst = cont ? slot_ptr(a, c, 0, tb) : a.C + (size_t)r * a.ldc + tb;
+#pragma unroll
+                for (int g = 0; g < 32 / U; ++g) {
+                    int cc[U];
+                    float vv[U];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        cc[u] = __shfl_sync(kFull, ccur, g * U + u);
+                        vv[u] = __shfl_sync(kFull, vcur, g * U + u);
+                    }
+                    float b[U][VL];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) ld_b<TB, VL>(b[u], Bl + (size_t)cc[u] * a.ldb);
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+#pragma unroll
+                        for (int e = 0; e < VL; ++e) acc[e] = fmaf(vv[u], b[u][e], acc[e]);
+                        if ((ends >> (g * U + u)) & 1u) {
+                            if constexpr (SCALED) {
+#pragma unroll
+                                for (int e = 0; e < VL; ++e) acc[e] *= sc[e];
+                            }
+                            st_hint<VL>(cdst, acc, pol_once);
+#pragma unroll
+                            for (int e = 0; e < VL; ++e) acc[e] = 0.0f;
+                            cont = false;
+                            ++r;
+                            cdst = a.C + (size_t)r * a.ldc + tb;
+                        }
+                    }
+                    // keep the next group's loads behind this group (registers)
+                    asm volatile("" ::: "memory");
+                }
+                ccur = cnext;
+                vcur = vnext;
+            }
+            // every row of [m0.y, s1) has been stored; row s1 may continue
+            bool tail_piece = false;
+            if (r < a.nr && r == s1 && __ldg(a.rowPtr + r) < k1) {
+                if constexpr (SCALED) {
+#pragma unroll
+                    for (int e = 0; e < VL; ++e) acc[e] *= sc[e];
+                }
+                tail_piece = !cont;  // a continuing row here is the head piece itself
+                st_v<VL>(slot_ptr(a, c, cont ? 0 : 1, tb), acc);
+            }
+            if (head_piece)
+                piece_arrive_ool<VL>(a.rowPtr, a.cnt, a.slots, a.C, a.ldc, a.nv, a.chunk, 0.0f,
+                                     m0.y, tb);
+            if (tail_piece)
+                piece_arrive_ool<VL>(a.rowPtr, a.cnt, a.slots, a.C, a.ldc, a.nv, a.chunk, 0.0f,
+                                     s1, tb);
+        }
+        unsigned int nx = 0;
+        if (lane == 0) nx = atomicAdd(a.head + blockIdx.y, 1u);
+        cl = nwarps + (long long)__shfl_sync(kFull, nx, 0);
+    }
+}
+
+// The lean pair: for beta == 0 without Kahan rows, k_bal_fast over every
+// chunk and k_bal_lean over the chunks it listed; otherwise k_bal_lean over
+// every chunk.  Grids: the CTAs that fit at once (chunks are handed out by
+// the queue), and one CTA per SM for the listed chunks.
+template <int W, typename TV, typename TB, bool K>
+inline void launch_lean(const Resolved &r, KArgs a, cudaStream_t st)
+{
+    const long long resident = (long long)device_sms() * DASPMM_LEAN_MINB;
+    const unsigned gx = (unsigned)std::max<long long>(
+        1, std::min<long long>(((long long)a.nchunks + 7) / 8, resident));
+    if (!K && a.beta == 0.0f) {
+        a.list_mode = 0;
+        k_bal_fast<W, DASPMM_LEAN_U, TV, TB><<<dim3(gx, r.tiles), 256, 0, st>>>(a);
+        a.list_mode = 1;
+        const unsigned gw = std::min<unsigned>(gx, (unsigned)device_sms());
+        k_bal_lean<W, DASPMM_LEAN_U, TV, TB, K><<<dim3(gw, r.tiles), 256, 0, st>>>(a);
+        count_launches(1);
+    } else {
+        a.list_mode = 0;
+        k_bal_lean<W, DASPMM_LEAN_U, TV, TB, K><<<dim3(gx, r.tiles), 256, 0, st>>>(a);
     }
 }
 

@@ -55,6 +55,12 @@ daspmm_status run_resolved(const Resolved &r, int layout, int nr, int nc, int nn
                            const int *rowPtr, const int *rowIdx, const int *colIdx,
                            const float *values, const float *B, float *C, float beta,
                            void *ws, size_t ws_bytes, cudaStream_t st);
+// Balanced CSR: the workspace's boundary table, split-row counters, chunk
+// queue heads and carry slots, and the partition launch that fills them.
+struct KArgs;
+void carve_balanced(const Resolved &r, void *ws, KArgs *a);
+void launch_partition(const Resolved &r, int nr, int nnz, const int *rowPtr, const KArgs &a,
+                      cudaStream_t st);
 daspmm_status cached_workspace(size_t need, cudaStream_t st, void **out);
 daspmm_status cached_host_staging(size_t need, cudaStream_t st, void **out);
 

@@ -53,6 +53,9 @@ struct KArgs {
     int *own;           // ownership recording (tests): [nr][2]
     int *cnt;           // pieces arrived per split row and column tile, at the
                         // row's first chunk: [nchunks][tiles]
+    unsigned int *head; // lean kernel: chunks handed out per column tile [tiles]
+    int *list;          // chunks the fast kernel left to the walk: [0] count, then ids
+    int list_mode;      // walk kernel: 0 every chunk (queue), 1 the listed ones
     const float *bscale;  // FP8 B: per-column scales
     int kahan_min;        // rows at least this long use compensated sums
 };
@@ -546,12 +549,16 @@ __global__ void __launch_bounds__(256) k_fix_coo(const KArgs a)
 // threshold that straddle chunk boundaries.
 // ======================================================================
 static __global__ void k_partition(int nr, int nnz, const int *__restrict__ rowPtr,
-                            int chunk, int snap, int nchunks, int2 *meta, int *cnt, int tiles)
+                            int chunk, int snap, int nchunks, int2 *meta, int *cnt, int tiles,
+                            unsigned int *head, int *list)
 {
     const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (r == 0) {
         meta[0] = make_int2(0, 0);
         meta[nchunks] = make_int2(nnz, nr);
+        if (head)
+            for (int t = 0; t < tiles; ++t) head[t] = 0;
+        if (list) list[0] = 0;
     }
     if (r >= nr) return;
     const int rs = __ldg(rowPtr + r), re = __ldg(rowPtr + r + 1);
@@ -617,6 +624,25 @@ __device__ __forceinline__ void piece_arrive(const KArgs &a, int row, int col)
         for (int e = 0; e < VL; ++e) tot[e] = fmaf(a.beta, old[e], tot[e]);
     }
     st_v<VL>(dst, tot);
+}
+
+// piece_arrive out of line, for kernels whose main loop needs every register
+// (split rows are a small fraction of the rows).
+template <int VL>
+__device__ __noinline__ void piece_arrive_ool(const int *__restrict__ rowPtr, int *cnt,
+                                              const float *slots, float *C, int ldc, int nv,
+                                              int chunk, float beta, int row, int col)
+{
+    KArgs a{};
+    a.rowPtr = rowPtr;
+    a.cnt = cnt;
+    a.slots = const_cast<float *>(slots);
+    a.C = C;
+    a.ldc = ldc;
+    a.nv = nv;
+    a.chunk = chunk;
+    a.beta = beta;
+    piece_arrive<VL>(a, row, col);
 }
 
 template <bool CM, int V, int CF, bool RECORD>

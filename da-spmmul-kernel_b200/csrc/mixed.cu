@@ -15,10 +15,7 @@ namespace daspmm {
 template <int W, typename TV, typename TB, bool K>
 static void launch_mixed_w(const Resolved &r, const KArgs &a, cudaStream_t st)
 {
-    const long long resident = (long long)device_sms() * DASPMM_LEAN_MINB;
-    const unsigned gx = (unsigned)std::max<long long>(
-        1, std::min<long long>(((long long)a.nchunks + 7) / 8, resident));
-    k_bal_lean<W, DASPMM_LEAN_U, TV, TB, K><<<dim3(gx, r.tiles), 256, 0, st>>>(a);
+    launch_lean<W, TV, TB, K>(r, a, st);
 }
 
 template <typename TV, typename TB>
@@ -145,14 +142,8 @@ daspmm_status daspmm_spmm_mixed(const daspmm_config *cfg_in, int layout, int nr,
     a.L = r.L; a.S = 1; a.chunk = r.chunk; a.nchunks = r.nchunks;
     a.bscale = b_scales;
     a.kahan_min = kahan_min > 0 ? kahan_min : 0x7fffffff;
-    int2 *meta = (int2 *)workspace;
-    char *p = (char *)workspace + align256(sizeof(int2) * ((size_t)r.nchunks + 1));
-    a.meta = meta;
-    a.cnt = (int *)p;
-    a.slots = (float *)(p + align256(sizeof(int) * (size_t)r.nchunks * r.tiles));
-    k_partition<<<(unsigned)std::max(1, (nr + 255) / 256), 256, 0, st>>>(
-        nr, nnz, rowPtr, r.chunk, r.snap, r.nchunks, meta, a.cnt, r.tiles);
-    count_launches(1);
+    carve_balanced(r, workspace, &a);
+    launch_partition(r, nr, nnz, rowPtr, a, st);
     const bool kahan = kahan_min > 0;
     timer_before(st);
     if (val_fmt == DASPMM_F32 && b_fmt == DASPMM_F32) launch_mixed<float, float>(r, a, kahan, st);
