@@ -353,7 +353,7 @@ def run_ours(args):
                        "parallelism": f"row shards x{world}, B replicated, no collective"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4),
-                         "traffic": traffic, "kernel": "k_bal_lean (main gather kernel)",
+                         "traffic": traffic, "kernel": "k_bal_fast + k_bal_lean list mode (main gather pair)",
                          "kernel_ms": round(kern_ms, 5), "algorithmic_bytes": abytes,
                          "peak_source": peak_src},
             "step_hbm_gbs": round(abytes / (ms_step * 1e-3) / 1e9, 1),
