@@ -300,7 +300,10 @@ static void launch_all(const Resolved &r, KArgs &a, dim3 grid, dim3 fix_grid, in
                        cudaStream_t st)
 {
     const bool fix = a.nchunks > 1;
-    timer_before(st);
+    // the lean pair's timing starts before k_partition (run_resolved), so no
+    // event sits between kernels that overlap by programmatic launch
+    const bool lean = r.alg == DASPMM_ALG_CSR_BALANCED && r.pipe == 4;
+    if (!lean) timer_before(st);
     switch (r.alg) {
     case DASPMM_ALG_CSR_SCALAR:
     case DASPMM_ALG_CSR_VECTOR:
@@ -420,6 +423,7 @@ daspmm_status run_resolved(const Resolved &r, int layout, int nr, int nc, int nn
         a.slots = (float *)ws;
     } else if (r.alg == DASPMM_ALG_CSR_BALANCED) {
         carve_balanced(r, ws, &a);
+        if (r.pipe == 4) timer_before(st);
         launch_partition(r, nr, nnz, rowPtr, a, st);
     }
     const long long units =

@@ -113,6 +113,7 @@ __global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_lean(const KArgs 
 #pragma unroll
     for (int e = 0; e < VL; ++e) sc[e] = SCALED ? __ldg(a.bscale + tb + e) : 1.0f;
 
+    pdl_wait();  // the boundaries (k_partition) or the list (k_bal_fast) are complete
     // Queue mode: chunks are handed out dynamically -- each warp starts with
     // chunk = its index, then takes the next unclaimed one from the column
     // tile's queue head (zeroed by k_partition), so warps that draw short
@@ -270,6 +271,8 @@ __global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_fast(const KArgs 
 #pragma unroll
     for (int e = 0; e < VL; ++e) sc[e] = SCALED ? __ldg(a.bscale + tb + e) : 1.0f;
 
+    pdl_trigger();  // the list-mode walk may be scheduled; it waits for this grid
+    pdl_wait();     // the boundaries from k_partition are complete
     long long cl = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     while (cl < a.nchunks) {
         const int c = (int)cl;
@@ -380,6 +383,25 @@ __global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_fast(const KArgs 
 // chunk and k_bal_lean over the chunks it listed; otherwise k_bal_lean over
 // every chunk.  Grids: the CTAs that fit at once (chunks are handed out by
 // the queue), and one CTA per SM for the listed chunks.
+// A launch that may overlap the previous kernel of the stream (programmatic
+// dependent launch); the kernel calls pdl_wait() before reading its inputs.
+// A failure is left in the runtime's last error for the caller's check.
+template <typename... P>
+inline void launch_pdl(void (*kernel)(P...), dim3 grid, cudaStream_t st, P... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 template <int W, typename TV, typename TB, bool K>
 inline void launch_lean(const Resolved &r, KArgs a, cudaStream_t st)
 {
@@ -388,14 +410,14 @@ inline void launch_lean(const Resolved &r, KArgs a, cudaStream_t st)
         1, std::min<long long>(((long long)a.nchunks + 7) / 8, resident));
     if (!K && a.beta == 0.0f) {
         a.list_mode = 0;
-        k_bal_fast<W, DASPMM_LEAN_U, TV, TB><<<dim3(gx, r.tiles), 256, 0, st>>>(a);
+        launch_pdl(k_bal_fast<W, DASPMM_LEAN_U, TV, TB>, dim3(gx, r.tiles), st, a);
         a.list_mode = 1;
         const unsigned gw = std::min<unsigned>(gx, (unsigned)device_sms());
-        k_bal_lean<W, DASPMM_LEAN_U, TV, TB, K><<<dim3(gw, r.tiles), 256, 0, st>>>(a);
+        launch_pdl(k_bal_lean<W, DASPMM_LEAN_U, TV, TB, K>, dim3(gw, r.tiles), st, a);
         count_launches(1);
     } else {
         a.list_mode = 0;
-        k_bal_lean<W, DASPMM_LEAN_U, TV, TB, K><<<dim3(gx, r.tiles), 256, 0, st>>>(a);
+        launch_pdl(k_bal_lean<W, DASPMM_LEAN_U, TV, TB, K>, dim3(gx, r.tiles), st, a);
     }
 }
 

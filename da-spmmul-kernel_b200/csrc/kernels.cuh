@@ -552,6 +552,7 @@ static __global__ void k_partition(int nr, int nnz, const int *__restrict__ rowP
                             int chunk, int snap, int nchunks, int2 *meta, int *cnt, int tiles,
                             unsigned int *head, int *list)
 {
+    asm volatile("griddepcontrol.launch_dependents;");  // the gather may be scheduled now
     const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (r == 0) {
         meta[0] = make_int2(0, 0);

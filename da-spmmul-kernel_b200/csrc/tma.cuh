@@ -65,6 +65,14 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
     return false;
 }
 
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialisation may start before the previous kernel of its stream has
+// finished; pdl_wait() blocks until that kernel has completed and its writes
+// are visible (a no-op for a kernel launched the ordinary way), and
+// pdl_trigger() lets the next kernel of the stream be scheduled early.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;"); }
+
 // Order this thread's earlier generic-proxy shared-memory accesses before
 // later async-proxy (bulk copy) writes to the same memory.
 __device__ __forceinline__ void fence_proxy_async_smem()
