@@ -589,9 +589,11 @@ __device__ __forceinline__ int last_chunk(int re, int chunk) { return (re - 1) /
 // it is counted at the row's first chunk and, if it is the last piece to
 // arrive, the warp adds all pieces in chunk order (the first chunk's tail,
 // then the heads) and stores the row: C = sum + beta*C.  VL floats per lane
-// at column `col`; all lanes of the warp call it.
+// at column `col`; all lanes of the warp call it.  tiles / tile: the column
+// tiles of the product and the one this piece belongs to.
 template <int VL>
-__device__ __forceinline__ void piece_arrive(const KArgs &a, int row, int col)
+__device__ __forceinline__ void piece_arrive(const KArgs &a, int row, int col, int tiles,
+                                             int tile)
 {
     const int rs = __ldg(a.rowPtr + row), re = __ldg(a.rowPtr + row + 1);
     const int c0 = first_chunk(rs, a.chunk), c1 = last_chunk(re, a.chunk);
@@ -599,7 +601,7 @@ __device__ __forceinline__ void piece_arrive(const KArgs &a, int row, int col)
     __syncwarp();
     int last = 0;
     if ((threadIdx.x & 31) == 0)  // one counter per (row, column tile)
-        last = atomicAdd(a.cnt + (size_t)c0 * gridDim.y + blockIdx.y, 1) == c1 - c0;
+        last = atomicAdd(a.cnt + (size_t)c0 * tiles + tile, 1) == c1 - c0;
     last = __shfl_sync(kFull, last, 0);
     if (!last) return;
     __threadfence();
@@ -632,7 +634,8 @@ __device__ __forceinline__ void piece_arrive(const KArgs &a, int row, int col)
 template <int VL>
 __device__ __noinline__ void piece_arrive_ool(const int *__restrict__ rowPtr, int *cnt,
                                               const float *slots, float *C, int ldc, int nv,
-                                              int chunk, float beta, int row, int col)
+                                              int chunk, float beta, int row, int col,
+                                              int tiles, int tile)
 {
     KArgs a{};
     a.rowPtr = rowPtr;
@@ -643,7 +646,7 @@ __device__ __noinline__ void piece_arrive_ool(const int *__restrict__ rowPtr, in
     a.nv = nv;
     a.chunk = chunk;
     a.beta = beta;
-    piece_arrive<VL>(a, row, col);
+    piece_arrive<VL>(a, row, col, tiles, tile);
 }
 
 template <bool CM, int V, int CF, bool RECORD>
