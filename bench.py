@@ -552,28 +552,29 @@ def run_serving(D, dev, seconds: float = 1.0, rate: float = 20000.0):
     return out
 
 
-def run_e2e(D, A, B, dev, alg, steps, pg=None):
+def run_e2e(D, A, B, dev, alg, steps, pg=None, nstreams=2):
     """Same SpMM through the host-buffer entry point: every step copies its
     inputs (rowPtr, colIdx, values, B) from pinned host memory to the device,
-    runs the SpMM and copies C back to pinned host memory.  Steps alternate
-    between two streams (daspmm_spmm_host_async, each stream with its own
+    runs the SpMM and copies C back to pinned host memory.  Steps rotate over
+    `nstreams` streams (daspmm_spmm_host_async, each stream with its own
     device staging and host C), so one step's C download overlaps the next
-    step's upload; timed with CUDA events around all steps (both streams
+    steps' uploads; timed with CUDA events around all steps (every stream
     joined), max over ranks."""
     import torch
     L = D.lib()
     pin = lambda a: torch.from_numpy(a).pin_memory()
     rp, ci, va, Bh = pin(A.rowPtr), pin(A.colIdx), pin(A.values), pin(B)
-    Ch = [torch.empty(A.nr * NV, dtype=torch.float32).pin_memory() for _ in range(2)]
+    Ch = [torch.empty(A.nr * NV, dtype=torch.float32).pin_memory() for _ in range(nstreams)]
     cfg = D.default_config(alg, 0, A.nr, A.nc, A.nnz, NV)
-    streams = [torch.cuda.Stream(dev), torch.cuda.Stream(dev)]
+    streams = [torch.cuda.Stream(dev) for _ in range(nstreams)]
 
     def once(i):
+        k = i % nstreams
         D.check(L.daspmm_spmm_host_async(
             ctypes.byref(cfg), 0, A.nr, A.nc, A.nnz, NV, ctypes.c_void_p(rp.data_ptr()), None,
             ctypes.c_void_p(ci.data_ptr()), ctypes.c_void_p(va.data_ptr()),
-            ctypes.c_void_p(Bh.data_ptr()), ctypes.c_void_p(Ch[i % 2].data_ptr()), 0.0,
-            ctypes.c_void_p(streams[i % 2].cuda_stream)), "spmm_host_async")
+            ctypes.c_void_p(Bh.data_ptr()), ctypes.c_void_p(Ch[k].data_ptr()), 0.0,
+            ctypes.c_void_p(streams[k].cuda_stream)), "spmm_host_async")
     for i in range(4):
         once(i)
     torch.cuda.synchronize(dev)
@@ -582,10 +583,12 @@ def run_e2e(D, A, B, dev, alg, steps, pg=None):
     torch.cuda.synchronize(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(streams[0])
-    streams[1].wait_event(e0)
+    for st in streams[1:]:
+        st.wait_event(e0)
     for i in range(steps):
         once(i)
-    streams[0].wait_stream(streams[1])
+    for st in streams[1:]:
+        streams[0].wait_stream(st)
     e1.record(streams[0])
     e1.synchronize()
     ms = e0.elapsed_time(e1) / steps
