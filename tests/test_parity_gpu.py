@@ -183,7 +183,7 @@ def test_balanced_tma_ring(mats, name):
     A, dA = mats[name]
     rng = np.random.default_rng(12)
     for pipe in (2, 3, 4):   # TMA ring / cp.async ring / lean register gather
-        for nv in (32, 64, 96, 128, 160, 256):
+        for nv in (32, 64, 96, 128, 160, 192, 256):
             B = rng.uniform(-1, 1, A.nc * nv).astype(np.float32)
             for kw in ({}, dict(chunk=40, snap=9), dict(chunk=7, snap=3), dict(chunk=5000),
                        dict(lanes_col=8, chunk=50)):   # 32-float tiles
@@ -206,7 +206,7 @@ def test_deterministic_repeat(mats):
         c1 = _run(A, dA, alg, 0, 32, B)
         c2 = _run(A, dA, alg, 0, 32, B)
         np.testing.assert_array_equal(c1, c2)
-    for pipe in (1, 2):
+    for pipe in (1, 2, 4):
         cfg = lambda: D.Config(alg=int(D.Alg.CSR_BALANCED), pipe=pipe, chunk=64)
         c1 = _run(A, dA, D.Alg.CSR_BALANCED, 0, 32, B, cfg=cfg())
         c2 = _run(A, dA, D.Alg.CSR_BALANCED, 0, 32, B, cfg=cfg())
