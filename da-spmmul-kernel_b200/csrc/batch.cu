@@ -55,8 +55,8 @@ static __global__ void k_batch_plan(const BatchInst *__restrict__ inst,
 // windowed gather over whole rows (no carries).  Lanes whose columns lie at or
 // past nv (nv % W != 0) load a clamped, in-bounds vector and store nothing.
 template <int W, int U, typename TV, typename TB>
-__device__ __forceinline__ void batch_rows(const BatchInst &I, int row0, int row1, int tb0,
-                                           uint64_t pol_once)
+__device__ __noinline__ void batch_rows(const BatchInst &I, int row0, int row1, int tb0,
+                                        uint64_t pol_once)
 {
     constexpr int VL = W / 32;
     constexpr bool SCALED = std::is_same<TB, fp8>::value;
@@ -144,6 +144,82 @@ __device__ __forceinline__ void batch_rows(const BatchInst &I, int row0, int row
     while (r < row1) {  // rows ending at k1, trailing empty rows included
         emit(r);
         ++r;
+    }
+}
+
+// Rows [row0, row1) of one instance, none of them empty, beta == 0: the ends
+// of the rows finishing in a window of 32 nonzeros come as one bitmask (lane l
+// looks at the end of row r + l; with no empty row the 32 lanes cover every
+// row that can end in the window), so the window is summed straight through
+// and a row is stored at its bit.  Same sums, in the same order, as
+// batch_rows.
+template <int W, int U, typename TV, typename TB>
+__device__ __forceinline__ void batch_rows_fast(const BatchInst &I, int row0, int row1,
+                                                int tb0, uint64_t pol_once)
+{
+    constexpr int VL = W / 32;
+    constexpr bool SCALED = std::is_same<TB, fp8>::value;
+    const int lane = threadIdx.x & 31;
+    const int col = tb0 + lane * VL;
+    const bool active = col < I.nv;
+    const int colc = active ? col : I.nv - VL;  // nv % VL == 0 (checked on the host)
+    const TB *Bl = reinterpret_cast<const TB *>(I.B) + colc;
+    const TV *Av = reinterpret_cast<const TV *>(I.vals);
+    const int k0 = __ldg(I.rowPtr + row0), k1 = __ldg(I.rowPtr + row1);
+    int r = row0;
+    int E = __ldg(I.rowPtr + min(r + 1 + lane, I.nr));
+    float acc[VL];
+#pragma unroll
+    for (int e = 0; e < VL; ++e) acc[e] = 0.0f;
+    auto load_win = [&](int wb, int &cc, float &vv) {
+        const bool ok = wb + lane < k1;
+        cc = ok ? ld_hint_s32(I.colIdx + wb + lane, pol_once) : 0;
+        vv = ok ? ld_val<TV>(Av + wb + lane, pol_once) : 0.0f;
+    };
+    int ccur, cnext;
+    float vcur, vnext;
+    load_win(k0, ccur, vcur);
+    for (int wb = k0; wb < k1; wb += 32) {
+        load_win(wb + 32, cnext, vnext);
+        const int cnt = min(32, k1 - wb);
+        const int pos = E - 1 - wb;
+        const bool in = r + lane < row1 && pos >= 0 && pos < cnt;
+        const unsigned ends = __reduce_or_sync(kFull, in ? (1u << pos) : 0u);
+        E = __ldg(I.rowPtr + min(r + __popc(ends) + 1 + lane, I.nr));  // next window's
+        float *cdst = I.C + (size_t)r * I.ldc + col;
+#pragma unroll
+        for (int g = 0; g < 32 / U; ++g) {
+            int cc[U];
+            float vv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                cc[u] = __shfl_sync(kFull, ccur, g * U + u);
+                vv[u] = __shfl_sync(kFull, vcur, g * U + u);
+            }
+            float b[U][VL];
+#pragma unroll
+            for (int u = 0; u < U; ++u) ld_b<TB, VL>(b[u], Bl + (size_t)cc[u] * I.ldb);
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+#pragma unroll
+                for (int e = 0; e < VL; ++e) acc[e] = fmaf(vv[u], b[u][e], acc[e]);
+                if ((ends >> (g * U + u)) & 1u) {
+                    if (active) {
+                        if constexpr (SCALED) {
+#pragma unroll
+                            for (int e = 0; e < VL; ++e) acc[e] *= __ldg(I.bscale + col + e);
+                        }
+                        st_hint<VL>(cdst, acc, pol_once);
+                    }
+#pragma unroll
+                    for (int e = 0; e < VL; ++e) acc[e] = 0.0f;
+                    ++r;
+                    cdst += I.ldc;
+                }
+            }
+        }
+        ccur = cnext;
+        vcur = vnext;
     }
 }
 
@@ -236,8 +312,12 @@ template <int W, typename TV, typename TB>
 __device__ __forceinline__ void batch_item(const BatchInst &I, const BatchTile &T, int ct,
                                            uint64_t pol_once)
 {
-    if (T.piece < 0) batch_rows<W, DASPMM_LEAN_U, TV, TB>(I, T.row0, T.row1, ct * W, pol_once);
-    else batch_piece<W, DASPMM_LEAN_U, TV, TB>(I, T, ct, pol_once);
+    if (T.piece >= 0)
+        batch_piece<W, DASPMM_LEAN_U, TV, TB>(I, T, ct, pol_once);
+    else if (T.npieces == 0 && I.beta == 0.0f)  // a run without empty rows
+        batch_rows_fast<W, DASPMM_LEAN_U, TV, TB>(I, T.row0, T.row1, ct * W, pol_once);
+    else
+        batch_rows<W, DASPMM_LEAN_U, TV, TB>(I, T.row0, T.row1, ct * W, pol_once);
 }
 
 // WM: the tile width every instance uses, or 0 for a batch of mixed widths
@@ -357,6 +437,8 @@ void build_tiles(const int *rp, int nr, int chunk, TilePlan *out)
         t.row1 = r;
         t.k0 = rp[t.row0];
         t.k1 = rp[r];
+        t.npieces = 0;  // a run: its number of empty rows
+        for (int q = t.row0; q < r; ++q) t.npieces += rp[q + 1] == rp[q];
         out->tiles.push_back(t);
     }
 }

@@ -81,7 +81,7 @@ struct BatchTile {
     int row0, row1;   // rows [row0, row1); a piece has row1 = row0 + 1
     int k0, k1;       // piece: nonzeros [k0, k1)
     int piece;        // -1 for a run of whole rows, else the piece index
-    int npieces;      // pieces of the row
+    int npieces;      // piece: pieces of the row; run: its empty rows
     int slot;         // piece: slot of piece 0 (slots slot .. slot+npieces-1)
     int cnt;          // piece: the row's counter index
 };
