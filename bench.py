@@ -137,6 +137,12 @@ def algorithmic_bytes(A, nv: int, s_val=4, s_b=4, s_c=4) -> int:
             + A.nr * nv * s_c)
 
 
+def gather_bytes(A, nv: int, s_val=4, s_b=4, s_c=4) -> int:
+    """The gather upper bound: every nonzero reads its whole B row from
+    memory (no reuse in any cache), C written once."""
+    return A.nnz * (4 + s_val) + 4 * (A.nr + 1) + A.nnz * nv * s_b + A.nr * nv * s_c
+
+
 def cpu_reference_time(A, B, nv, nthreads, reps, row_sample=None):
     """ms per pass of the reference's cpuSpmvReference (or the oracle port)."""
     import numpy as np
@@ -331,6 +337,8 @@ def run_ours(args):
                    "cores": cores, "kind": kind,
                    "sample": f"full matrix ({nnz_s} nnz, N=128), median of 3 passes, 1 thread"}
         mixed = None if args.no_mixed else run_mixed(D, A, dA, B, dev, K, peak)
+        if mixed is not None and world == 1:
+            mixed["random_1m_deg8"] = run_mixed_random(D, dev, peak)
         batched = None if (args.no_batched or world > 1) else run_batched(D, dev)
         serving = None if (args.no_serving or world > 1) else run_serving(D, dev, args.serve_seconds)
         clk = sampler.summary()
@@ -355,6 +363,7 @@ def run_ours(args):
                          "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "traffic": traffic, "kernel": "k_bal_fast + k_bal_lean list mode (main gather pair)",
                          "kernel_ms": round(kern_ms, 5), "algorithmic_bytes": abytes,
+                         "gather_upper_bound_bytes": gather_bytes(A, NV),
                          "peak_source": peak_src},
             "step_hbm_gbs": round(abytes / (ms_step * 1e-3) / 1e9, 1),
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": int(launches),
@@ -405,6 +414,55 @@ def run_mixed(D, A, dA, B, dev, steps, peak):
                      "ms_per_step": round(ms, 5), "kernel_ms": round(kms, 5),
                      "algorithmic_bytes": abytes,
                      "roofline_frac": round(abytes / (kms * 1e-3) / 1e9 / peak, 4)}
+    return out
+
+
+def run_mixed_random(D, dev, peak, steps: int = 10):
+    """The second mixed-precision matrix: 1,048,576 rows, uniform random
+    columns, average degree 8 (Poisson row lengths, seed 0); N in {32, 128,
+    512}; FP32, BF16 values and B, BF16 values + E4M3 B.  Device time of the
+    SpMM per call (library timer), GFLOP/s and the fraction of the measured
+    HBM copy bandwidth its algorithmic bytes reach."""
+    import torch
+    L = D.lib()
+    A = D.gen_random(1 << 20, 1 << 20, 8.0, seed=0)
+    dA = D.DeviceCsr(A, dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(0)
+    vq = D.quantize(dA.values, D.Fmt.BF16)
+    out = {"nr": A.nr, "nnz": A.nnz}
+    for nv in (32, 128, 512):
+        Bt = torch.empty(A.nc * nv, device=dev).uniform_(-1, 1, generator=g)
+        C = torch.zeros(A.nr * nv, dtype=torch.float32, device=dev)
+        b16 = D.quantize(Bt, D.Fmt.BF16)
+        sc = D.e4m3_scales(Bt, A.nc, nv)
+        b8 = D.quantize(Bt, D.Fmt.E4M3, sc, nv)
+        runs = {
+            "f32": (lambda: D.spmm(D.Alg.CSR_BALANCED, 0, dA, Bt, C, nv=nv), 4, 4),
+            "bf16": (lambda: D.spmm_mixed(dA, vq, D.Fmt.BF16, b16, D.Fmt.BF16, C, nv), 2, 2),
+            "bf16_e4m3": (lambda: D.spmm_mixed(dA, vq, D.Fmt.BF16, b8, D.Fmt.E4M3, C, nv,
+                                               b_scales=sc), 2, 1),
+        }
+        res = {}
+        for name, (run, s_val, s_b) in runs.items():
+            for _ in range(3):
+                run()
+            torch.cuda.synchronize(dev)
+            D.check(L.daspmm_kernel_timer_begin(steps), "kernel_timer_begin")
+            for _ in range(steps):
+                run()
+            torch.cuda.synchronize(dev)
+            kt = (ctypes.c_float * steps)()
+            n = L.daspmm_kernel_timer_end(kt, steps)
+            kms = sum(kt) / max(1, n)
+            abytes = algorithmic_bytes(A, nv, s_val=s_val, s_b=s_b) + (4 * nv if s_b == 1 else 0)
+            gbytes = gather_bytes(A, nv, s_val=s_val, s_b=s_b)
+            res[name] = {"gflops": round(2.0 * A.nnz * nv / (kms * 1e-3) / 1e9, 1),
+                         "ms": round(kms, 4),
+                         "roofline_frac": round(abytes / (kms * 1e-3) / 1e9 / peak, 4),
+                         "gather_bound_frac": round(gbytes / (kms * 1e-3) / 1e9 / peak, 4)}
+        out[f"n{nv}"] = res
+        del Bt, C, b16, b8
     return out
 
 
