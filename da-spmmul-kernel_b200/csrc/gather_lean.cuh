@@ -401,6 +401,221 @@ __global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_fast(const KArgs 
     }
 }
 
+// ---------------------------------------------------------------- half-warp form
+// 8 consecutive floats (32 bytes, 32-byte aligned).
+__device__ __forceinline__ void ld8_nc(float (&r)[8], const float *p)
+{
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(r[0]), "=f"(r[1]), "=f"(r[2]), "=f"(r[3]), "=f"(r[4]), "=f"(r[5]), "=f"(r[6]),
+          "=f"(r[7])
+        : "l"(p));
+}
+__device__ __forceinline__ void ld8_cg(float (&r)[8], const float *p)
+{
+    asm volatile("ld.global.cg.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=f"(r[0]), "=f"(r[1]), "=f"(r[2]), "=f"(r[3]), "=f"(r[4]), "=f"(r[5]),
+                   "=f"(r[6]), "=f"(r[7])
+                 : "l"(p)
+                 : "memory");
+}
+__device__ __forceinline__ void st8(float *p, const float (&r)[8])
+{
+    asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "f"(r[0]),
+                 "f"(r[1]), "f"(r[2]), "f"(r[3]), "f"(r[4]), "f"(r[5]), "f"(r[6]), "f"(r[7])
+                 : "memory");
+}
+__device__ __forceinline__ void st8_hint(float *p, const float (&r)[8], uint64_t pol)
+{
+    asm volatile("st.global.L2::cache_hint.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8}, %9;" ::
+                     "l"(p), "f"(r[0]), "f"(r[1]), "f"(r[2]), "f"(r[3]), "f"(r[4]), "f"(r[5]),
+                 "f"(r[6]), "f"(r[7]), "l"(pol)
+                 : "memory");
+}
+
+// piece_arrive for a 16-lane half of a warp (lanes of `hmask`, 8 floats per
+// lane at column `col`), beta == 0: the same counters, carries and order of
+// summation as piece_arrive, so the two combine pieces of one row freely.
+static __device__ __noinline__ void piece_arrive_half(const int *__restrict__ rowPtr, int *cnt,
+                                               const float *slots, float *C, int ldc, int nv,
+                                               int chunk, int row, int col, int tiles, int tile,
+                                               unsigned hmask)
+{
+    const int rs = __ldg(rowPtr + row), re = __ldg(rowPtr + row + 1);
+    const int c0 = first_chunk(rs, chunk), c1 = last_chunk(re, chunk);
+    __threadfence();
+    __syncwarp(hmask);
+    int last = 0;
+    if ((threadIdx.x & 15) == 0) last = atomicAdd(cnt + (size_t)c0 * tiles + tile, 1) == c1 - c0;
+    last = __shfl_sync(hmask, last, 0, 16);
+    if (!last) return;
+    __threadfence();
+    float tot[8];
+    ld8_cg(tot, slots + ((size_t)c0 * 2 + 1) * nv + col);
+    constexpr int P = 2;  // independent carry loads in flight
+    for (int cb = c0 + 1; cb <= c1; cb += P) {
+        float hp[P][8];
+#pragma unroll
+        for (int u = 0; u < P; ++u)
+            if (cb + u <= c1) ld8_cg(hp[u], slots + ((size_t)(cb + u) * 2) * nv + col);
+#pragma unroll
+        for (int u = 0; u < P; ++u)
+            if (cb + u <= c1)
+#pragma unroll
+                for (int e = 0; e < 8; ++e) tot[e] += hp[u][e];
+    }
+    st8(C + (size_t)row * ldc + col, tot);
+}
+
+#ifndef DASPMM_HALF
+#define DASPMM_HALF 1       // FP32 128-column tiles take the half-warp kernel
+#endif
+#ifndef DASPMM_HALF_U
+#define DASPMM_HALF_U 8     // nonzeros in flight per half-warp step
+#endif
+#ifndef DASPMM_HALF_MINB
+#define DASPMM_HALF_MINB 2  // CTAs of 256 threads per SM: 16 warps, <= 128 registers
+#endif
+
+// k_bal_fast with a 16-lane worker: FP32, 128-column tiles, beta == 0, B and C
+// 32-byte aligned.  Each half of a warp takes one chunk of a pair (2p, 2p+1)
+// and covers a B row of 128 floats with 16 lanes x 32-byte loads, so one warp
+// instruction gathers two nonzeros -- half the instructions per nonzero of
+// the 32-lane form and twice the bytes in flight per warp.  The halves run in
+// step: the window loop runs to the longer chunk of the pair (balanced chunks
+// differ by a few nonzeros), a half past its chunk's end is predicated off.
+// Windows are 16 nonzeros (lane l of a half ends row r + l), the rest is
+// k_bal_fast's: same chunks, carries, split-row combine and order of
+// summation, so results are bit-identical to it.
+template <int U>
+__global__ void __launch_bounds__(256, DASPMM_HALF_MINB) k_bal_half(const KArgs a)
+{
+    constexpr int VL = 8;
+    const int lane = threadIdx.x & 31, h = lane >> 4, hl = lane & 15;
+    const unsigned hmask = 0xFFFFu << (16 * h);
+    const int tile = blockIdx.y, tiles = gridDim.y;
+    const int tb = tile * 128 + hl * VL;
+    const float *Bl = a.B + tb;
+    const uint64_t pol_once = policy_evict_first();
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const long long npairs = ((long long)a.nchunks + 1) >> 1;
+
+    pdl_trigger();  // the list-mode walk may be scheduled; it waits for this grid
+    pdl_wait();     // the boundaries from k_partition are complete
+    long long pl = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    while (pl < npairs) {
+        const int c = (int)(2 * pl) + h;
+        const bool have = c < a.nchunks;
+        int k0 = 0, k1 = 0, s1 = 0, r = 0, rstart = 0;
+        if (have) {
+            const int2 m0 = a.meta[c], m1 = a.meta[c + 1];
+            k0 = m0.x;
+            k1 = m1.x;
+            s1 = m1.y;
+            r = m0.y;
+            rstart = __ldg(a.rowPtr + r);
+        }
+        const int r0 = r;
+        // ends of rows r .. r+15; any empty row among [r, s1) hands the chunk on
+        int E = __ldg(a.rowPtr + min(r + 1 + hl, a.nr));
+        bool empty_row;
+        {
+            int prev = __shfl_up_sync(kFull, E, 1, 16);
+            if (hl == 0) prev = rstart;
+            empty_row = (__ballot_sync(kFull, have && r + hl < s1 && E == prev) & hmask) != 0;
+            int last = __shfl_sync(kFull, E, 15, 16);
+            bool more = have && !empty_row && r + 16 < s1;
+            for (int rb = r + 16; __any_sync(kFull, more); rb += 16) {
+                int e2 = 0;
+                if (more) e2 = __ldg(a.rowPtr + min(rb + 1 + hl, a.nr));
+                int p2 = __shfl_up_sync(kFull, e2, 1, 16);
+                if (hl == 0) p2 = last;
+                const unsigned b2 = __ballot_sync(kFull, more && rb + hl < s1 && e2 == p2);
+                if (more) empty_row = (b2 & hmask) != 0;
+                last = __shfl_sync(kFull, e2, 15, 16);
+                more = more && !empty_row && rb + 16 < s1;
+            }
+        }
+        const bool skip = !have || empty_row;
+        if (have && empty_row && tile == 0 && hl == 0) a.list[1 + atomicAdd(a.list, 1)] = c;
+        const int kb = skip ? 0 : k0, ke = skip ? 0 : k1;
+        int nwin = (ke - kb + 15) >> 4;
+        nwin = max(nwin, __shfl_xor_sync(kFull, nwin, 16));
+        bool cont = !skip && k0 > rstart;
+        const bool head_piece = cont;
+        float acc[VL];
+#pragma unroll
+        for (int e = 0; e < VL; ++e) acc[e] = 0.0f;
+        auto load_win = [&](int wb, int &col, float &val) {
+            const bool ok = wb + hl < ke;
+            col = ok ? ld_hint_s32(a.colIdx + wb + hl, pol_once) : 0;
+            val = ok ? ld_hint_f32(a.vals + wb + hl, pol_once) : 0.0f;
+        };
+        int ccur, cnext;
+        float vcur, vnext;
+        int wb = kb;
+        load_win(wb, ccur, vcur);
+        for (int w = 0; w < nwin; ++w, wb += 16) {
+            load_win(wb + 16, cnext, vnext);
+            const int cnt = ke - wb;  // nonzeros of this half left (<= 0: idle)
+            const int pos = E - 1 - wb;
+            const bool in = r + 1 + hl <= a.nr && pos >= 0 && pos < min(cnt, 16);
+            const unsigned e32 = __reduce_or_sync(kFull, in ? (1u << (pos + 16 * h)) : 0u);
+            const unsigned ends = (e32 >> (16 * h)) & 0xFFFFu;
+            // the next window's row ends load while this one is summed
+            E = __ldg(a.rowPtr + min(r + __popc(ends) + 1 + hl, a.nr));
+            float *cdst = cont ? slot_ptr(a, c, 0, tb) : a.C + (size_t)r * a.ldc + tb;
+#pragma unroll
+            for (int g = 0; g < 16 / U; ++g) {
+                int cc[U];
+                float vv[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    cc[u] = __shfl_sync(kFull, ccur, g * U + u, 16);
+                    vv[u] = __shfl_sync(kFull, vcur, g * U + u, 16);
+                }
+                float b[U][VL];
+#pragma unroll
+                for (int u = 0; u < U; ++u) ld8_nc(b[u], Bl + (size_t)cc[u] * a.ldb);
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    // positions past the chunk's end add nothing (not even 0 * B)
+                    if (g * U + u < cnt) {
+#pragma unroll
+                        for (int e = 0; e < VL; ++e) acc[e] = fmaf(vv[u], b[u][e], acc[e]);
+                    }
+                    if ((ends >> (g * U + u)) & 1u) {
+                        st8_hint(cdst, acc, pol_once);
+#pragma unroll
+                        for (int e = 0; e < VL; ++e) acc[e] = 0.0f;
+                        cont = false;
+                        ++r;
+                        cdst = a.C + (size_t)r * a.ldc + tb;
+                    }
+                }
+                asm volatile("" ::: "memory");
+            }
+            ccur = cnext;
+            vcur = vnext;
+        }
+        // every row of [m0.y, s1) has been stored; row s1 may continue
+        bool tail_piece = false;
+        if (!skip && r < a.nr && r == s1 && __ldg(a.rowPtr + r) < k1) {
+            tail_piece = !cont;  // a continuing row here is the head piece itself
+            st8(slot_ptr(a, c, cont ? 0 : 1, tb), acc);
+        }
+        if (head_piece)
+            piece_arrive_half(a.rowPtr, a.cnt, a.slots, a.C, a.ldc, a.nv, a.chunk, r0, tb, tiles,
+                              tile, hmask);
+        if (tail_piece)
+            piece_arrive_half(a.rowPtr, a.cnt, a.slots, a.C, a.ldc, a.nv, a.chunk, s1, tb, tiles,
+                              tile, hmask);
+        __syncwarp();
+        unsigned int nx = 0;
+        if (lane == 0) nx = atomicAdd(a.head + tile, 1u);
+        pl = nwarps + (long long)__shfl_sync(kFull, nx, 0);
+    }
+}
+
 // The lean pair: for beta == 0 without Kahan rows, k_bal_fast over every
 // chunk and k_bal_lean over the chunks it listed; otherwise k_bal_lean over
 // every chunk.  Grids: the CTAs that fit at once (chunks are handed out by
@@ -432,7 +647,17 @@ inline void launch_lean(const Resolved &r, KArgs a, cudaStream_t st)
         1, std::min<long long>(((long long)a.nchunks + 7) / 8, resident));
     if (!K && a.beta == 0.0f) {
         a.list_mode = 0;
-        if constexpr (W == 128) {
+        constexpr bool f32 = std::is_same<TV, float>::value && std::is_same<TB, float>::value;
+        const bool al32 = ((reinterpret_cast<uintptr_t>(a.B) | reinterpret_cast<uintptr_t>(a.C) |
+                            reinterpret_cast<uintptr_t>(a.slots)) & 31) == 0 &&
+                          a.ldb % 8 == 0 && a.ldc % 8 == 0 && a.nv % 8 == 0;
+        if (W == 128 && f32 && DASPMM_HALF && al32) {
+            const long long pairs = ((long long)a.nchunks + 1) / 2;
+            const unsigned gh = (unsigned)std::max<long long>(
+                1, std::min<long long>((pairs + 7) / 8,
+                                       (long long)device_sms() * DASPMM_HALF_MINB));
+            launch_pdl(k_bal_half<DASPMM_HALF_U>, dim3(gh, r.tiles), st, a);
+        } else if constexpr (W == 128) {
             launch_pdl(k_bal_fast<W, DASPMM_LEAN_U, TV, TB>, dim3(gx, r.tiles), st, a);
         } else {  // one queue of (tile, chunk) items
             const long long items = (long long)a.nchunks * r.tiles;
