@@ -205,7 +205,11 @@ daspmm_status resolve(const daspmm_config *cfg, int layout, int nr, int nc, int 
             r.block = r.pipe == 4 ? 256 : 128;
             if (!cfg->chunk) {
                 if (r.pipe == 4) {
-                    r.chunk = 128;  // measured best on the power-law benchmark matrix
+                    // measured on the 262k power-law and 1M random matrices: one
+                    // 128-column tile runs best at 96 nonzeros per chunk (FP32
+                    // 93.3 -> 88.6 us on the power-law matrix), wider products
+                    // (several tiles in flight) at 128
+                    r.chunk = nv == 128 ? 96 : 128;
                 } else {
                     // rings: one wave of chunks over the resident warps (12 per SM)
                     const long long slots = (long long)device_sms() * 12;

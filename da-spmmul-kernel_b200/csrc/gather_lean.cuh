@@ -38,16 +38,50 @@ using bf16 = __nv_bfloat16;
 using fp16 = __half;
 using fp8 = __nv_fp8_e4m3;
 
+// 8 consecutive floats (32 bytes, 32-byte aligned).
+__device__ __forceinline__ void ld8_nc(float (&r)[8], const float *p)
+{
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(r[0]), "=f"(r[1]), "=f"(r[2]), "=f"(r[3]), "=f"(r[4]), "=f"(r[5]), "=f"(r[6]),
+          "=f"(r[7])
+        : "l"(p));
+}
+__device__ __forceinline__ void ld8_cg(float (&r)[8], const float *p)
+{
+    asm volatile("ld.global.cg.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=f"(r[0]), "=f"(r[1]), "=f"(r[2]), "=f"(r[3]), "=f"(r[4]), "=f"(r[5]),
+                   "=f"(r[6]), "=f"(r[7])
+                 : "l"(p)
+                 : "memory");
+}
+__device__ __forceinline__ void st8(float *p, const float (&r)[8])
+{
+    asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "f"(r[0]),
+                 "f"(r[1]), "f"(r[2]), "f"(r[3]), "f"(r[4]), "f"(r[5]), "f"(r[6]), "f"(r[7])
+                 : "memory");
+}
+__device__ __forceinline__ void st8_hint(float *p, const float (&r)[8], uint64_t pol)
+{
+    asm volatile("st.global.L2::cache_hint.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8}, %9;" ::
+                     "l"(p), "f"(r[0]), "f"(r[1]), "f"(r[2]), "f"(r[3]), "f"(r[4]), "f"(r[5]),
+                 "f"(r[6]), "f"(r[7]), "l"(pol)
+                 : "memory");
+}
+
 // N consecutive elements of B (storage type T) as floats, one vector load.
 template <typename T, int N>
 __device__ __forceinline__ void ld_b(float (&r)[N], const T *p)
 {
     if constexpr (std::is_same<T, float>::value) {
-        ld_nc<N>(r, reinterpret_cast<const float *>(p));
+        if constexpr (N == 8) ld8_nc(r, reinterpret_cast<const float *>(p));
+        else ld_nc<N>(r, reinterpret_cast<const float *>(p));
     } else if constexpr (sizeof(T) == 2) {
-        // 2-byte types: N = 4 -> 8 bytes, 2 -> 4 bytes, 1 -> 2 bytes
+        // 2-byte types: N = 8 -> 16 bytes, 4 -> 8 bytes, 2 -> 4 bytes, 1 -> 2 bytes
         uint32_t w[(N + 1) / 2];
-        if constexpr (N == 4) {
+        if constexpr (N == 8) {
+            const uint4 t = __ldg(reinterpret_cast<const uint4 *>(p));
+            w[0] = t.x; w[1] = t.y; w[2] = t.z; w[3] = t.w;
+        } else if constexpr (N == 4) {
             const uint2 t = __ldg(reinterpret_cast<const uint2 *>(p));
             w[0] = t.x; w[1] = t.y;
         } else if constexpr (N == 2) {
@@ -62,14 +96,21 @@ __device__ __forceinline__ void ld_b(float (&r)[N], const T *p)
             else r[i] = __half2float(__ushort_as_half(h));
         }
     } else {  // fp8 e4m3: N bytes
-        uint32_t w;
-        if constexpr (N == 4) w = __ldg(reinterpret_cast<const unsigned int *>(p));
-        else if constexpr (N == 2) w = __ldg(reinterpret_cast<const unsigned short *>(p));
-        else w = __ldg(reinterpret_cast<const unsigned char *>(p));
+        uint32_t w[(N + 3) / 4];
+        if constexpr (N == 8) {
+            const uint2 t = __ldg(reinterpret_cast<const uint2 *>(p));
+            w[0] = t.x; w[1] = t.y;
+        } else if constexpr (N == 4) {
+            w[0] = __ldg(reinterpret_cast<const unsigned int *>(p));
+        } else if constexpr (N == 2) {
+            w[0] = __ldg(reinterpret_cast<const unsigned short *>(p));
+        } else {
+            w[0] = __ldg(reinterpret_cast<const unsigned char *>(p));
+        }
 #pragma unroll
         for (int i = 0; i < N; i += 2) {
-            const __half2_raw h2 =
-                __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(w >> (8 * i)), __NV_E4M3);
+            const __half2_raw h2 = __nv_cvt_fp8x2_to_halfraw2(
+                (__nv_fp8x2_storage_t)(w[i / 4] >> (8 * (i % 4))), __NV_E4M3);
             const float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&h2));
             r[i] = f.x;
             if (i + 1 < N) r[i + 1] = f.y;
@@ -402,39 +443,10 @@ __global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_fast(const KArgs 
 }
 
 // ---------------------------------------------------------------- half-warp form
-// 8 consecutive floats (32 bytes, 32-byte aligned).
-__device__ __forceinline__ void ld8_nc(float (&r)[8], const float *p)
-{
-    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-        : "=f"(r[0]), "=f"(r[1]), "=f"(r[2]), "=f"(r[3]), "=f"(r[4]), "=f"(r[5]), "=f"(r[6]),
-          "=f"(r[7])
-        : "l"(p));
-}
-__device__ __forceinline__ void ld8_cg(float (&r)[8], const float *p)
-{
-    asm volatile("ld.global.cg.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                 : "=f"(r[0]), "=f"(r[1]), "=f"(r[2]), "=f"(r[3]), "=f"(r[4]), "=f"(r[5]),
-                   "=f"(r[6]), "=f"(r[7])
-                 : "l"(p)
-                 : "memory");
-}
-__device__ __forceinline__ void st8(float *p, const float (&r)[8])
-{
-    asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "f"(r[0]),
-                 "f"(r[1]), "f"(r[2]), "f"(r[3]), "f"(r[4]), "f"(r[5]), "f"(r[6]), "f"(r[7])
-                 : "memory");
-}
-__device__ __forceinline__ void st8_hint(float *p, const float (&r)[8], uint64_t pol)
-{
-    asm volatile("st.global.L2::cache_hint.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8}, %9;" ::
-                     "l"(p), "f"(r[0]), "f"(r[1]), "f"(r[2]), "f"(r[3]), "f"(r[4]), "f"(r[5]),
-                 "f"(r[6]), "f"(r[7]), "l"(pol)
-                 : "memory");
-}
-
 // piece_arrive for a 16-lane half of a warp (lanes of `hmask`, 8 floats per
 // lane at column `col`), beta == 0: the same counters, carries and order of
 // summation as piece_arrive, so the two combine pieces of one row freely.
+template <typename TV, typename TB>  // one copy per kernel (ptxas 12.9 faults on a shared one)
 static __device__ __noinline__ void piece_arrive_half(const int *__restrict__ rowPtr, int *cnt,
                                                const float *slots, float *C, int ldc, int nv,
                                                int chunk, int row, int col, int tiles, int tile,
@@ -486,15 +498,20 @@ static __device__ __noinline__ void piece_arrive_half(const int *__restrict__ ro
 // Windows are 16 nonzeros (lane l of a half ends row r + l), the rest is
 // k_bal_fast's: same chunks, carries, split-row combine and order of
 // summation, so results are bit-identical to it.
-template <int U>
+template <int U, typename TV = float, typename TB = float>
 __global__ void __launch_bounds__(256, DASPMM_HALF_MINB) k_bal_half(const KArgs a)
 {
     constexpr int VL = 8;
+    constexpr bool SCALED = std::is_same<TB, fp8>::value;
     const int lane = threadIdx.x & 31, h = lane >> 4, hl = lane & 15;
     const unsigned hmask = 0xFFFFu << (16 * h);
     const int tile = blockIdx.y, tiles = gridDim.y;
     const int tb = tile * 128 + hl * VL;
-    const float *Bl = a.B + tb;
+    const TB *Bl = reinterpret_cast<const TB *>(a.B) + tb;
+    const TV *Av = reinterpret_cast<const TV *>(a.vals);
+    float sc[VL];
+#pragma unroll
+    for (int e = 0; e < VL; ++e) sc[e] = SCALED ? __ldg(a.bscale + tb + e) : 1.0f;
     const uint64_t pol_once = policy_evict_first();
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     const long long npairs = ((long long)a.nchunks + 1) >> 1;
@@ -548,7 +565,7 @@ __global__ void __launch_bounds__(256, DASPMM_HALF_MINB) k_bal_half(const KArgs 
         auto load_win = [&](int wb, int &col, float &val) {
             const bool ok = wb + hl < ke;
             col = ok ? ld_hint_s32(a.colIdx + wb + hl, pol_once) : 0;
-            val = ok ? ld_hint_f32(a.vals + wb + hl, pol_once) : 0.0f;
+            val = ok ? ld_val<TV>(Av + wb + hl, pol_once) : 0.0f;
         };
         int ccur, cnext;
         float vcur, vnext;
@@ -575,7 +592,7 @@ __global__ void __launch_bounds__(256, DASPMM_HALF_MINB) k_bal_half(const KArgs 
                 }
                 float b[U][VL];
 #pragma unroll
-                for (int u = 0; u < U; ++u) ld8_nc(b[u], Bl + (size_t)cc[u] * a.ldb);
+                for (int u = 0; u < U; ++u) ld_b<TB, VL>(b[u], Bl + (size_t)cc[u] * a.ldb);
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
                     // positions past the chunk's end add nothing (not even 0 * B)
@@ -584,6 +601,10 @@ __global__ void __launch_bounds__(256, DASPMM_HALF_MINB) k_bal_half(const KArgs 
                         for (int e = 0; e < VL; ++e) acc[e] = fmaf(vv[u], b[u][e], acc[e]);
                     }
                     if ((ends >> (g * U + u)) & 1u) {
+                        if constexpr (SCALED) {
+#pragma unroll
+                            for (int e = 0; e < VL; ++e) acc[e] *= sc[e];
+                        }
                         st8_hint(cdst, acc, pol_once);
 #pragma unroll
                         for (int e = 0; e < VL; ++e) acc[e] = 0.0f;
@@ -601,13 +622,17 @@ __global__ void __launch_bounds__(256, DASPMM_HALF_MINB) k_bal_half(const KArgs 
         bool tail_piece = false;
         if (!skip && r < a.nr && r == s1 && __ldg(a.rowPtr + r) < k1) {
             tail_piece = !cont;  // a continuing row here is the head piece itself
+            if constexpr (SCALED) {
+#pragma unroll
+                for (int e = 0; e < VL; ++e) acc[e] *= sc[e];
+            }
             st8(slot_ptr(a, c, cont ? 0 : 1, tb), acc);
         }
         if (head_piece)
-            piece_arrive_half(a.rowPtr, a.cnt, a.slots, a.C, a.ldc, a.nv, a.chunk, r0, tb, tiles,
+            piece_arrive_half<TV, TB>(a.rowPtr, a.cnt, a.slots, a.C, a.ldc, a.nv, a.chunk, r0, tb, tiles,
                               tile, hmask);
         if (tail_piece)
-            piece_arrive_half(a.rowPtr, a.cnt, a.slots, a.C, a.ldc, a.nv, a.chunk, s1, tb, tiles,
+            piece_arrive_half<TV, TB>(a.rowPtr, a.cnt, a.slots, a.C, a.ldc, a.nv, a.chunk, s1, tb, tiles,
                               tile, hmask);
         __syncwarp();
         unsigned int nx = 0;
@@ -647,16 +672,21 @@ inline void launch_lean(const Resolved &r, KArgs a, cudaStream_t st)
         1, std::min<long long>(((long long)a.nchunks + 7) / 8, resident));
     if (!K && a.beta == 0.0f) {
         a.list_mode = 0;
+        // the half-warp kernel: 8 elements of B per lane (one 8 * sizeof(TB)
+        // byte load), 32-byte stores of C and carries
+        const bool aligned8 =
+            (reinterpret_cast<uintptr_t>(a.B) % (8 * sizeof(TB))) == 0 &&
+            ((reinterpret_cast<uintptr_t>(a.C) | reinterpret_cast<uintptr_t>(a.slots)) & 31) == 0 &&
+            a.ldb % 8 == 0 && a.ldc % 8 == 0 && a.nv % 8 == 0;
         constexpr bool f32 = std::is_same<TV, float>::value && std::is_same<TB, float>::value;
-        const bool al32 = ((reinterpret_cast<uintptr_t>(a.B) | reinterpret_cast<uintptr_t>(a.C) |
-                            reinterpret_cast<uintptr_t>(a.slots)) & 31) == 0 &&
-                          a.ldb % 8 == 0 && a.ldc % 8 == 0 && a.nv % 8 == 0;
-        if (W == 128 && f32 && DASPMM_HALF && al32) {
+        // measured: the half-warp form wins for FP32 storage only (BF16 / E4M3
+        // B: 16 / 8-byte lane loads, slower than k_bal_fast)
+        if (W == 128 && f32 && DASPMM_HALF && aligned8) {
             const long long pairs = ((long long)a.nchunks + 1) / 2;
             const unsigned gh = (unsigned)std::max<long long>(
                 1, std::min<long long>((pairs + 7) / 8,
                                        (long long)device_sms() * DASPMM_HALF_MINB));
-            launch_pdl(k_bal_half<DASPMM_HALF_U>, dim3(gh, r.tiles), st, a);
+            if constexpr (f32) launch_pdl(k_bal_half<DASPMM_HALF_U>, dim3(gh, r.tiles), st, a);
         } else if constexpr (W == 128) {
             launch_pdl(k_bal_fast<W, DASPMM_LEAN_U, TV, TB>, dim3(gx, r.tiles), st, a);
         } else {  // one queue of (tile, chunk) items

@@ -45,6 +45,8 @@ def test_abi_version_and_status_strings():
 def test_default_configs():
     c = D.default_config(D.Alg.CSR_BALANCED, D.Layout.ROW_MAJOR, 262144, 262144, 1_227_000, 128)
     assert (c.vec, c.lanes_col, c.lanes_nnz, c.cf, c.pipe) == (4, 32, 1, 1, 4)
+    assert c.chunk == 96 and c.snap == 48 and c.block == 256   # one 128-column tile
+    c = D.default_config(D.Alg.CSR_BALANCED, D.Layout.ROW_MAJOR, 262144, 262144, 1_227_000, 512)
     assert c.chunk == 128 and c.snap == 64 and c.block == 256
     # the TMA ring sizes one wave of chunks over 148 SMs x 12 warps (no GPU here: 148)
     r = D.Config(alg=4, pipe=2)
