@@ -323,6 +323,17 @@ __global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_fast(const KArgs 
 
     pdl_trigger();  // the list-mode walk may be scheduled; it waits for this grid
     pdl_wait();     // the boundaries from k_partition are complete
+    // A chunk's last window is padded with column 0, value 0: that adds
+    // nothing unless row 0 of B holds an Inf or NaN (0 * Inf = NaN).  Then
+    // every chunk is handed to the walk kernel, which never pads (the same
+    // decision in every warp and column tile).
+    bool pad_ok = true;
+    for (int k = lane; k < a.nv; k += 32) {
+        float x[1];
+        ld_b<TB, 1>(x, reinterpret_cast<const TB *>(a.B) + k);
+        pad_ok &= isfinite(x[0]);
+    }
+    pad_ok = __all_sync(kFull, pad_ok);
     long long cl = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     while (cl < limit) {
         int tile, c;
@@ -359,7 +370,7 @@ __global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_fast(const KArgs 
                 last = __shfl_sync(kFull, e2, 31);
             }
         }
-        if (empty_row) {
+        if (empty_row || !pad_ok) {
             if (tile == 0 && lane == 0) a.list[1 + atomicAdd(a.list, 1)] = c;  // every tile
         } else {
             bool cont = k0 > rstart;

@@ -289,3 +289,28 @@ def test_full_size_configs(cuda):
     for alg in (D.Alg.CSR_BALANCED, D.Alg.CSR_SCALAR, D.Alg.COO_SCALAR):
         C = _run(A2, d2, alg, 0, nv, B)
         _check(A2, 0, nv, B, C, what=f"cfg2 {alg.name}")
+
+
+def test_half_warp_kernel_equals_32_lane_kernel(cuda):
+    """FP32 128-column tiles: with B and C 32-byte aligned the half-warp window
+    kernel runs, with both 16 bytes off that alignment the 32-lane one.  Same
+    chunks and order of summation: the products are bit-identical."""
+    import torch
+    rng = np.random.default_rng(12)
+    for A in (D.gen_powerlaw(20000, dmax=2000, seed=8), D.gen_random(5000, 4000, 5.0, seed=9)):
+        dA = D.DeviceCsr(A)
+        for nv in (128, 256):
+            B = rng.uniform(-1, 1, A.nc * nv).astype(np.float32)
+            Ba = torch.from_numpy(B).cuda()
+            Ca = torch.empty(A.nr * nv, device="cuda")
+            Bbuf = torch.zeros(A.nc * nv + 8, device="cuda")
+            Cbuf = torch.zeros(A.nr * nv + 8, device="cuda")
+            Bo, Co = Bbuf[4:4 + A.nc * nv], Cbuf[4:4 + A.nr * nv]
+            assert Ba.data_ptr() % 32 == 0 and Ca.data_ptr() % 32 == 0
+            assert Bo.data_ptr() % 32 == 16 and Co.data_ptr() % 32 == 16
+            Bo.copy_(Ba)
+            D.spmm(D.Alg.CSR_BALANCED, D.Layout.ROW_MAJOR, dA, Ba, Ca, nv=nv)
+            D.spmm(D.Alg.CSR_BALANCED, D.Layout.ROW_MAJOR, dA, Bo, Co, nv=nv)
+            torch.cuda.synchronize()
+            assert torch.equal(Ca, Co), f"nr={A.nr} nv={nv}: the two window kernels differ"
+            _check(A, 0, nv, B, Ca.cpu().numpy(), what=f"half-warp nv={nv}")
