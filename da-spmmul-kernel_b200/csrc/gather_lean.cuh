@@ -505,8 +505,9 @@ static __device__ __noinline__ void piece_arrive_half(const int *__restrict__ ro
 // instruction gathers two nonzeros -- half the instructions per nonzero of
 // the 32-lane form and twice the bytes in flight per warp.  The halves run in
 // step: the window loop runs to the longer chunk of the pair (balanced chunks
-// differ by a few nonzeros), a half past its chunk's end is predicated off.
-// Windows are 16 nonzeros (lane l of a half ends row r + l), the rest is
+// differ by a few nonzeros); a half past its chunk's end gathers padding
+// (column 0, value 0) and stores nothing.  Windows are 16 nonzeros (lane l of
+// a half ends row r + l), the rest is
 // k_bal_fast's: same chunks, carries, split-row combine and order of
 // summation, so results are bit-identical to it.
 template <int U, typename TV = float, typename TB = float>
@@ -529,6 +530,15 @@ __global__ void __launch_bounds__(256, DASPMM_HALF_MINB) k_bal_half(const KArgs 
 
     pdl_trigger();  // the list-mode walk may be scheduled; it waits for this grid
     pdl_wait();     // the boundaries from k_partition are complete
+    // padding (column 0, value 0) adds nothing unless row 0 of B holds an Inf
+    // or NaN; then every chunk is handed to the walk kernel (as in k_bal_fast)
+    bool pad_ok = true;
+    for (int k = lane; k < a.nv; k += 32) {
+        float x[1];
+        ld_b<TB, 1>(x, reinterpret_cast<const TB *>(a.B) + k);
+        pad_ok &= isfinite(x[0]);
+    }
+    pad_ok = __all_sync(kFull, pad_ok);
     long long pl = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     while (pl < npairs) {
         const int c = (int)(2 * pl) + h;
@@ -563,8 +573,9 @@ __global__ void __launch_bounds__(256, DASPMM_HALF_MINB) k_bal_half(const KArgs 
                 more = more && !empty_row && rb + 16 < s1;
             }
         }
-        const bool skip = !have || empty_row;
-        if (have && empty_row && tile == 0 && hl == 0) a.list[1 + atomicAdd(a.list, 1)] = c;
+        const bool skip = !have || empty_row || !pad_ok;
+        if (have && (empty_row || !pad_ok) && tile == 0 && hl == 0)
+            a.list[1 + atomicAdd(a.list, 1)] = c;  // every tile
         const int kb = skip ? 0 : k0, ke = skip ? 0 : k1;
         int nwin = (ke - kb + 15) >> 4;
         nwin = max(nwin, __shfl_xor_sync(kFull, nwin, 16));
@@ -606,11 +617,8 @@ __global__ void __launch_bounds__(256, DASPMM_HALF_MINB) k_bal_half(const KArgs 
                 for (int u = 0; u < U; ++u) ld_b<TB, VL>(b[u], Bl + (size_t)cc[u] * a.ldb);
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
-                    // positions past the chunk's end add nothing (not even 0 * B)
-                    if (g * U + u < cnt) {
 #pragma unroll
-                        for (int e = 0; e < VL; ++e) acc[e] = fmaf(vv[u], b[u][e], acc[e]);
-                    }
+                    for (int e = 0; e < VL; ++e) acc[e] = fmaf(vv[u], b[u][e], acc[e]);
                     if ((ends >> (g * U + u)) & 1u) {
                         if constexpr (SCALED) {
 #pragma unroll

@@ -418,11 +418,12 @@ daspmm_status daspmm_spmm_host_async(const daspmm_config *cfg, int layout, int n
  * library or any other.
  *   - Limit: daspmm_workspace_bytes() of the DASPMM_ALG_CSR_BALANCED default
  *     configuration (daspmm_default_config) must be <= DASPMM_NOALLOC_MAX_BYTES.
- *     That is about 8 * nchunks * nv bytes: for row-major nv a multiple of 32
- *     the default makes one chunk per resident warp (12 per SM, 1776 on a
- *     148-SM B200), so nv up to about 1100 fits whatever nnz is; otherwise
- *     nchunks = ceil(nnz / 32..128).  Larger problems return
- *     DASPMM_ERR_WORKSPACE before any device work.
+ *     That is about 8 * nchunks * nv bytes (two carry rows per chunk), with
+ *     nchunks = ceil(nnz / chunk): chunk = 96 for nv = 128 and 128 for the
+ *     other row-major nv that are multiples of 32 (32..128 otherwise).  So
+ *     nv = 128 fits up to about 1.6 M nonzeros (the 262,144-row power-law
+ *     matrix, 1.24 M, needs 13.4 MB), nv = 32 about 8 M.  Larger problems
+ *     return DASPMM_ERR_WORKSPACE before any device work.
  *   - The first call on each device looks up the array's device address with
  *     that device current; make that first call before any stream capture.
  *   - All calls on a device share the one array.  Calls that overlap on the
