@@ -454,10 +454,30 @@ __global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_fast(const KArgs 
 }
 
 // ---------------------------------------------------------------- half-warp form
-// piece_arrive for a 16-lane half of a warp (lanes of `hmask`, 8 floats per
+// VL floats: plain / L2-hinted stores and L2-coherent loads, VL <= 8.
+template <int VL>
+__device__ __forceinline__ void st_n(float *p, const float (&r)[VL])
+{
+    if constexpr (VL == 8) st8(p, r);
+    else st_v<VL>(p, r);
+}
+template <int VL>
+__device__ __forceinline__ void st_hint_n(float *p, const float (&r)[VL], uint64_t pol)
+{
+    if constexpr (VL == 8) st8_hint(p, r, pol);
+    else st_hint<VL>(p, r, pol);
+}
+template <int VL>
+__device__ __forceinline__ void ld_cg_n(float (&r)[VL], const float *p)
+{
+    if constexpr (VL == 8) ld8_cg(r, p);
+    else ld_cg<VL>(r, p);
+}
+
+// piece_arrive for a 16-lane half of a warp (lanes of `hmask`, VL floats per
 // lane at column `col`), beta == 0: the same counters, carries and order of
 // summation as piece_arrive, so the two combine pieces of one row freely.
-template <typename TV, typename TB>  // one copy per kernel (ptxas 12.9 faults on a shared one)
+template <int VL, typename TV, typename TB>  // one copy per kernel (ptxas 12.9 faults on a shared one)
 static __device__ __noinline__ void piece_arrive_half(const int *__restrict__ rowPtr, int *cnt,
                                                const float *slots, float *C, int ldc, int nv,
                                                int chunk, int row, int col, int tiles, int tile,
@@ -472,21 +492,21 @@ static __device__ __noinline__ void piece_arrive_half(const int *__restrict__ ro
     last = __shfl_sync(hmask, last, 0, 16);
     if (!last) return;
     __threadfence();
-    float tot[8];
-    ld8_cg(tot, slots + ((size_t)c0 * 2 + 1) * nv + col);
+    float tot[VL];
+    ld_cg_n<VL>(tot, slots + ((size_t)c0 * 2 + 1) * nv + col);
     constexpr int P = 2;  // independent carry loads in flight
     for (int cb = c0 + 1; cb <= c1; cb += P) {
-        float hp[P][8];
+        float hp[P][VL];
 #pragma unroll
         for (int u = 0; u < P; ++u)
-            if (cb + u <= c1) ld8_cg(hp[u], slots + ((size_t)(cb + u) * 2) * nv + col);
+            if (cb + u <= c1) ld_cg_n<VL>(hp[u], slots + ((size_t)(cb + u) * 2) * nv + col);
 #pragma unroll
         for (int u = 0; u < P; ++u)
             if (cb + u <= c1)
 #pragma unroll
-                for (int e = 0; e < 8; ++e) tot[e] += hp[u][e];
+                for (int e = 0; e < VL; ++e) tot[e] += hp[u][e];
     }
-    st8(C + (size_t)row * ldc + col, tot);
+    st_n<VL>(C + (size_t)row * ldc + col, tot);
 }
 
 #ifndef DASPMM_HALF
@@ -497,6 +517,9 @@ static __device__ __noinline__ void piece_arrive_half(const int *__restrict__ ro
 #endif
 #ifndef DASPMM_HALF_MINB
 #define DASPMM_HALF_MINB 2  // CTAs of 256 threads per SM: 16 warps, <= 128 registers
+#endif
+#ifndef DASPMM_HALF4_MINB
+#define DASPMM_HALF4_MINB 3 // 64-column form (4 floats per lane): 24 warps, <= 80 registers
 #endif
 
 // k_bal_fast with a 16-lane worker: FP32, 128-column tiles, beta == 0, B and C
@@ -510,15 +533,15 @@ static __device__ __noinline__ void piece_arrive_half(const int *__restrict__ ro
 // a half ends row r + l), the rest is
 // k_bal_fast's: same chunks, carries, split-row combine and order of
 // summation, so results are bit-identical to it.
-template <int U, typename TV = float, typename TB = float>
-__global__ void __launch_bounds__(256, DASPMM_HALF_MINB) k_bal_half(const KArgs a)
+template <int U, int VL = 8, typename TV = float, typename TB = float>
+__global__ void __launch_bounds__(256, VL == 8 ? DASPMM_HALF_MINB : DASPMM_HALF4_MINB)
+    k_bal_half(const KArgs a)
 {
-    constexpr int VL = 8;
     constexpr bool SCALED = std::is_same<TB, fp8>::value;
     const int lane = threadIdx.x & 31, h = lane >> 4, hl = lane & 15;
     const unsigned hmask = 0xFFFFu << (16 * h);
     const int tile = blockIdx.y, tiles = gridDim.y;
-    const int tb = tile * 128 + hl * VL;
+    const int tb = tile * (16 * VL) + hl * VL;
     const TB *Bl = reinterpret_cast<const TB *>(a.B) + tb;
     const TV *Av = reinterpret_cast<const TV *>(a.vals);
     float sc[VL];
@@ -624,7 +647,7 @@ __global__ void __launch_bounds__(256, DASPMM_HALF_MINB) k_bal_half(const KArgs 
 #pragma unroll
                             for (int e = 0; e < VL; ++e) acc[e] *= sc[e];
                         }
-                        st8_hint(cdst, acc, pol_once);
+                        st_hint_n<VL>(cdst, acc, pol_once);
 #pragma unroll
                         for (int e = 0; e < VL; ++e) acc[e] = 0.0f;
                         cont = false;
@@ -645,13 +668,13 @@ __global__ void __launch_bounds__(256, DASPMM_HALF_MINB) k_bal_half(const KArgs 
 #pragma unroll
                 for (int e = 0; e < VL; ++e) acc[e] *= sc[e];
             }
-            st8(slot_ptr(a, c, cont ? 0 : 1, tb), acc);
+            st_n<VL>(slot_ptr(a, c, cont ? 0 : 1, tb), acc);
         }
         if (head_piece)
-            piece_arrive_half<TV, TB>(a.rowPtr, a.cnt, a.slots, a.C, a.ldc, a.nv, a.chunk, r0, tb, tiles,
+            piece_arrive_half<VL, TV, TB>(a.rowPtr, a.cnt, a.slots, a.C, a.ldc, a.nv, a.chunk, r0, tb, tiles,
                               tile, hmask);
         if (tail_piece)
-            piece_arrive_half<TV, TB>(a.rowPtr, a.cnt, a.slots, a.C, a.ldc, a.nv, a.chunk, s1, tb, tiles,
+            piece_arrive_half<VL, TV, TB>(a.rowPtr, a.cnt, a.slots, a.C, a.ldc, a.nv, a.chunk, s1, tb, tiles,
                               tile, hmask);
         __syncwarp();
         unsigned int nx = 0;
@@ -691,21 +714,25 @@ inline void launch_lean(const Resolved &r, KArgs a, cudaStream_t st)
         1, std::min<long long>(((long long)a.nchunks + 7) / 8, resident));
     if (!K && a.beta == 0.0f) {
         a.list_mode = 0;
-        // the half-warp kernel: 8 elements of B per lane (one 8 * sizeof(TB)
-        // byte load), 32-byte stores of C and carries
-        const bool aligned8 =
-            (reinterpret_cast<uintptr_t>(a.B) % (8 * sizeof(TB))) == 0 &&
-            ((reinterpret_cast<uintptr_t>(a.C) | reinterpret_cast<uintptr_t>(a.slots)) & 31) == 0 &&
-            a.ldb % 8 == 0 && a.ldc % 8 == 0 && a.nv % 8 == 0;
+        // the half-warp kernel: HV = W / 16 elements of B per lane (one
+        // HV * sizeof(TB) byte load), HV * 4-byte stores of C and carries
+        constexpr int HV = W / 16;
+        const bool aligned_h =
+            (reinterpret_cast<uintptr_t>(a.B) % (HV * sizeof(TB))) == 0 &&
+            ((reinterpret_cast<uintptr_t>(a.C) | reinterpret_cast<uintptr_t>(a.slots)) %
+             (HV * 4)) == 0 &&
+            a.ldb % HV == 0 && a.ldc % HV == 0 && a.nv % W == 0;
         constexpr bool f32 = std::is_same<TV, float>::value && std::is_same<TB, float>::value;
-        // measured: the half-warp form wins for FP32 storage only (BF16 / E4M3
-        // B: 16 / 8-byte lane loads, slower than k_bal_fast)
-        if (W == 128 && f32 && DASPMM_HALF && aligned8) {
+        // measured: the half-warp form wins for FP32 storage and 128-column
+        // tiles only (BF16 / E4M3 B: 16 / 8-byte lane loads; 64-column tiles
+        // (k_bal_half<U, 4>): 59.5 against 58.8 us at N = 64 -- k_bal_fast)
+        if (W == 128 && f32 && DASPMM_HALF && aligned_h) {
             const long long pairs = ((long long)a.nchunks + 1) / 2;
+            const long long minb = W == 128 ? DASPMM_HALF_MINB : DASPMM_HALF4_MINB;
             const unsigned gh = (unsigned)std::max<long long>(
-                1, std::min<long long>((pairs + 7) / 8,
-                                       (long long)device_sms() * DASPMM_HALF_MINB));
-            if constexpr (f32) launch_pdl(k_bal_half<DASPMM_HALF_U>, dim3(gh, r.tiles), st, a);
+                1, std::min<long long>((pairs + 7) / 8, (long long)device_sms() * minb));
+            if constexpr (f32 && W == 128)
+                launch_pdl(k_bal_half<DASPMM_HALF_U, HV>, dim3(gh, r.tiles), st, a);
         } else if constexpr (W == 128) {
             launch_pdl(k_bal_fast<W, DASPMM_LEAN_U, TV, TB>, dim3(gx, r.tiles), st, a);
         } else {  // one queue of (tile, chunk) items
