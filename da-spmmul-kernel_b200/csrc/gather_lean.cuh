@@ -501,7 +501,9 @@ __device__ __forceinline__ void ld_cg_n(float (&r)[VL], const float *p)
 // piece_arrive for a 16-lane half of a warp (lanes of `hmask`, VL floats per
 // lane at column `col`), beta == 0: the same counters, carries and order of
 // summation as piece_arrive, so the two combine pieces of one row freely.
-template <int VL, typename TV, typename TB>  // one copy per kernel (ptxas 12.9 faults on a shared one)
+// Templated on the kernel's types so that every kernel has its own copy:
+// ptxas 12.9 crashes (at build time) on one copy shared by two kernels.
+template <int VL, typename TV, typename TB>
 static __device__ __noinline__ void piece_arrive_half(const int *__restrict__ rowPtr, int *cnt,
                                                const float *slots, float *C, int ldc, int nv,
                                                int chunk, int row, int col, int tiles, int tile,
