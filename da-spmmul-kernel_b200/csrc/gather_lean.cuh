@@ -145,9 +145,6 @@ __device__ __forceinline__ float ld_val(const T *p, uint64_t pol)
 #ifndef DASPMM_LEAN_U
 #define DASPMM_LEAN_U 4     // nonzeros (B rows) in flight per warp step
 #endif
-#ifndef DASPMM_LEAN_PF
-#define DASPMM_LEAN_PF 0    // k_bal_fast: bulk L2 prefetch of the next window's B rows
-#endif
 
 template <int W, int U, typename TV = float, typename TB = float, bool KAHAN = false>
 __global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_lean(const KArgs a)
@@ -389,25 +386,8 @@ __global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_fast(const KArgs 
             int ccur, cnext;
             float vcur, vnext;
             load_win(k0, ccur, vcur);
-#if DASPMM_LEAN_PF
-            // B rows one window ahead go to L2 by a bulk prefetch (one row of
-            // W elements per lane; 16-byte aligned B only)
-            const bool pf = (reinterpret_cast<uintptr_t>(a.B) & 15) == 0;
-            load_win(k0 + 32, cnext, vnext);
-            int cn2;
-            float vn2;
-#endif
             for (int wb = k0; wb < k1; wb += 32) {
-#if DASPMM_LEAN_PF
-                if (pf && wb + 32 + lane < k1)
-                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(
-                                     reinterpret_cast<const TB *>(a.B) + tile * W +
-                                     (size_t)cnext * a.ldb),
-                                 "r"((int)(W * sizeof(TB))));
-                load_win(wb + 64, cn2, vn2);
-#else
                 load_win(wb + 32, cnext, vnext);
-#endif
                 const int cnt = min(32, k1 - wb);
                 const int pos = E - 1 - wb;
                 const bool in = r + 1 + lane <= a.nr && pos >= 0 && pos < cnt;
@@ -449,10 +429,6 @@ __global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_fast(const KArgs 
                 }
                 ccur = cnext;
                 vcur = vnext;
-#if DASPMM_LEAN_PF
-                cnext = cn2;
-                vnext = vn2;
-#endif
             }
             // every row of [m0.y, s1) has been stored; row s1 may continue
             bool tail_piece = false;
@@ -543,9 +519,6 @@ static __device__ __noinline__ void piece_arrive_half(const int *__restrict__ ro
 #endif
 #ifndef DASPMM_HALF_MINB
 #define DASPMM_HALF_MINB 2  // CTAs of 256 threads per SM: 16 warps, <= 128 registers
-#endif
-#ifndef DASPMM_HALF_PF
-#define DASPMM_HALF_PF 0    // bulk L2 prefetch of the next window's B rows
 #endif
 #ifndef DASPMM_HALF4_MINB
 #define DASPMM_HALF4_MINB 3 // 64-column form (4 floats per lane): 24 warps, <= 80 registers
@@ -645,34 +618,8 @@ __global__ void __launch_bounds__(256, VL == 8 ? DASPMM_HALF_MINB : DASPMM_HALF4
         float vcur, vnext;
         int wb = kb;
         load_win(wb, ccur, vcur);
-#if DASPMM_HALF_PF
-        // B rows DASPMM_HALF_PF windows ahead go to L2 by a bulk prefetch (one
-        // 16 * VL * 4-byte row per lane), so the window's own loads hit L2
-        load_win(wb + 16, cnext, vnext);
-        int cn2;
-        float vn2;
-#if DASPMM_HALF_PF == 2
-        load_win(wb + 32, cn2, vn2);
-        int cn3;
-        float vn3;
-#endif
-#endif
         for (int w = 0; w < nwin; ++w, wb += 16) {
-#if DASPMM_HALF_PF == 1
-            if (wb + 16 + hl < ke)
-                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(
-                                 Bl + (size_t)cnext * a.ldb),
-                             "r"(16 * VL * 4));
-            load_win(wb + 32, cn2, vn2);
-#elif DASPMM_HALF_PF == 2
-            if (wb + 32 + hl < ke)
-                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(
-                                 Bl + (size_t)cn2 * a.ldb),
-                             "r"(16 * VL * 4));
-            load_win(wb + 48, cn3, vn3);
-#else
             load_win(wb + 16, cnext, vnext);
-#endif
             const int cnt = ke - wb;  // nonzeros of this half left (<= 0: idle)
             const int pos = E - 1 - wb;
             const bool in = r + 1 + hl <= a.nr && pos >= 0 && pos < min(cnt, 16);
@@ -714,14 +661,6 @@ __global__ void __launch_bounds__(256, VL == 8 ? DASPMM_HALF_MINB : DASPMM_HALF4
             }
             ccur = cnext;
             vcur = vnext;
-#if DASPMM_HALF_PF
-            cnext = cn2;
-            vnext = vn2;
-#if DASPMM_HALF_PF == 2
-            cn2 = cn3;
-            vn2 = vn3;
-#endif
-#endif
         }
         // every row of [m0.y, s1) has been stored; row s1 may continue
         bool tail_piece = false;
