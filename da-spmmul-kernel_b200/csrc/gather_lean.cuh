@@ -520,9 +520,6 @@ static __device__ __noinline__ void piece_arrive_half(const int *__restrict__ ro
 #ifndef DASPMM_HALF_MINB
 #define DASPMM_HALF_MINB 2  // CTAs of 256 threads per SM: 16 warps, <= 128 registers
 #endif
-#ifndef DASPMM_HALF4_MINB
-#define DASPMM_HALF4_MINB 3 // 64-column form (4 floats per lane): 24 warps, <= 80 registers
-#endif
 
 // k_bal_fast with a 16-lane worker: FP32, 128-column tiles, beta == 0, B and C
 // 32-byte aligned.  Each half of a warp takes one chunk of a pair (2p, 2p+1)
@@ -536,8 +533,7 @@ static __device__ __noinline__ void piece_arrive_half(const int *__restrict__ ro
 // k_bal_fast's: same chunks, carries, split-row combine and order of
 // summation, so results are bit-identical to it.
 template <int U, int VL = 8, typename TV = float, typename TB = float>
-__global__ void __launch_bounds__(256, VL == 8 ? DASPMM_HALF_MINB : DASPMM_HALF4_MINB)
-    k_bal_half(const KArgs a)
+__global__ void __launch_bounds__(256, DASPMM_HALF_MINB) k_bal_half(const KArgs a)
 {
     constexpr bool SCALED = std::is_same<TB, fp8>::value;
     const int lane = threadIdx.x & 31, h = lane >> 4, hl = lane & 15;
@@ -730,9 +726,9 @@ inline void launch_lean(const Resolved &r, KArgs a, cudaStream_t st)
         // (k_bal_half<U, 4>): 59.5 against 58.8 us at N = 64 -- k_bal_fast)
         if (W == 128 && f32 && DASPMM_HALF && aligned_h) {
             const long long pairs = ((long long)a.nchunks + 1) / 2;
-            const long long minb = W == 128 ? DASPMM_HALF_MINB : DASPMM_HALF4_MINB;
             const unsigned gh = (unsigned)std::max<long long>(
-                1, std::min<long long>((pairs + 7) / 8, (long long)device_sms() * minb));
+                1, std::min<long long>((pairs + 7) / 8,
+                                       (long long)device_sms() * DASPMM_HALF_MINB));
             if constexpr (f32 && W == 128)
                 launch_pdl(k_bal_half<DASPMM_HALF_U, HV>, dim3(gh, r.tiles), st, a);
         } else if constexpr (W == 128) {
