@@ -368,7 +368,7 @@ def run_ours(args):
                        "parallelism": f"row shards x{world}, B replicated, no collective"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4),
-                         "traffic": traffic, "kernel": "k_bal_half + k_bal_lean list mode (main gather pair)",
+                         "traffic": traffic, "kernel": "k_bal_half (main gather; timed with k_partition and the k_bal_lean list walk)",
                          "kernel_ms": round(kern_ms, 5), "algorithmic_bytes": abytes,
                          "gather_upper_bound_bytes": gather_bytes(A, NV),
                          "peak_source": peak_src},
