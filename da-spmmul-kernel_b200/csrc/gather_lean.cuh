@@ -157,11 +157,10 @@ __global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_lean(const KArgs 
     const TB *Bl = reinterpret_cast<const TB *>(a.B) + tb;
     const TV *Av = reinterpret_cast<const TV *>(a.vals);
     const uint64_t pol_once = policy_evict_first();
-    float sc[VL];
+    pdl_wait();  // the boundaries (k_partition) or the list (k_bal_fast) are complete
+    float sc[VL];  // read after the wait, like every input
 #pragma unroll
     for (int e = 0; e < VL; ++e) sc[e] = SCALED ? __ldg(a.bscale + tb + e) : 1.0f;
-
-    pdl_wait();  // the boundaries (k_partition) or the list (k_bal_fast) are complete
     // Queue mode: chunks are handed out dynamically -- each warp starts with
     // chunk = its index, then takes the next unclaimed one from the column
     // tile's queue head (zeroed by k_partition), so warps that draw short
