@@ -48,6 +48,13 @@ def test_default_configs():
     assert c.chunk == 96 and c.snap == 48 and c.block == 256   # one 128-column tile
     c = D.default_config(D.Alg.CSR_BALANCED, D.Layout.ROW_MAJOR, 262144, 262144, 1_227_000, 512)
     assert c.chunk == 128 and c.snap == 64 and c.block == 256
+    # mixed precision keeps 128-nonzero chunks: never more workspace than the
+    # FP32 default a caller sizes it with
+    for nv in (32, 64, 128, 256, 512):
+        f32 = D.workspace_bytes(D.Config(alg=4), 0, 262144, 262144, 1_227_000, nv)
+        mixed = D.workspace_bytes(D.Config(alg=4, pipe=4, chunk=128), 0, 262144, 262144,
+                                  1_227_000, nv)
+        assert mixed <= f32, nv
     # the TMA ring sizes one wave of chunks over 148 SMs x 12 warps (no GPU here: 148)
     r = D.Config(alg=4, pipe=2)
     c = D.default_config(D.Alg.CSR_BALANCED, D.Layout.ROW_MAJOR, 262144, 262144, 1_227_000, 128)
