@@ -40,9 +40,18 @@ L2_BYTES = 126 * 1024 * 1024
 FALLBACK_HBM_GBS = 6650.0
 
 
-def workload_name(alg_name: str) -> str:
-    return (f"power-law graph 262144x262144 (~1.23M nnz, out-degree (k+0.16)^-2.1 on [1,4096], "
-            f"preferential attachment), B 262144x128 FP32 row-major, alg {alg_name}")
+WORKLOAD = "FP32 CSR SpMM, power-law graph 262144x262144 (seed 0), B 262144x128 row-major"
+
+
+def bench_config(nr: int, nnz: int, world: int) -> dict:
+    """The workload as both arms print it (identical keys and values)."""
+    return {"workload": WORKLOAD, "nr": nr, "nnz": nnz, "nv": NV,
+            "matrix": "out-degree (k+0.16)^-2.1 on [1,4096], preferential-attachment columns, "
+                      "values U(-1,1); B U(-1,1) seed 1",
+            "l2": "inputs larger than L2 (B 134 MB read + C 134 MB written per step > 126 MB), "
+                  "no flush between steps (part of B stays L2-resident from the step before)",
+            "parallelism": (f"row shards x{world}, B replicated, no collective" if world > 1
+                            else "single GPU")}
 
 
 def measured_peak():
@@ -177,13 +186,15 @@ def dist_env():
 
 # ---------------------------------------------------------------- reference arm
 def run_reference(args):
-    import numpy as np
-    import daspmm as D
+    # Inputs come from the oracle's restatement of the library's seeded
+    # generators (bit-identical, tests/test_oracle_gen.py): this arm loads
+    # only oracle/ libraries.
+    from oracle import oracle as O
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    A = D.gen_powerlaw(NR, seed=0)
-    B = D.gen_dense(A.nc * NV, seed=1)
+    A = O.gen_powerlaw(NR, seed=0)
+    B = O.gen_dense(A.nc * NV, seed=1)
     threads = os.cpu_count() or 1
     # calibrate: one full pass, then a row sample sized so W+K steps take ~60 s
     full_ms, _, _, kind, _ = cpu_reference_time(A, B, NV, threads, 1)
@@ -205,8 +216,8 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": workload_name("cpuSpmvReference (host)"), "nr": NR, "nv": NV,
-                   "nnz": A.nnz},
+        "config": bench_config(A.nr, A.nnz, args.gpus),
+        "variant": "cpuSpmvReference (spmvspmm_benchmark.cu:11-39), host",
         "cpu_baseline": {"value": round(gflops, 3), "unit": UNIT, "cores": cores, "kind": kind,
                          "sample": sample},
         "e2e": {"value": round(gflops, 3), "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -361,11 +372,8 @@ def run_ours(args):
             "steps": K, "warmup": args.warmup, "ms_per_step": round(ms_step, 5),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": workload_name(alg.name), "nr": A.nr, "nnz": A.nnz, "nv": NV,
-                       "variant": cfg_used.as_dict(),
-                       "l2": "inputs larger than L2 (working set %.0f MB > 126 MB), no flush"
-                             % (abytes / 1e6),
-                       "parallelism": f"row shards x{world}, B replicated, no collective"},
+            "config": bench_config(A.nr, A.nnz, world),
+            "variant": dict(cfg_used.as_dict(), alg_name=alg.name),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "traffic": traffic, "kernel": "k_bal_half (main gather; timed with k_partition and the k_bal_lean list walk)",

@@ -340,3 +340,161 @@ void or_dequantize(int fmt, size_t n, const void *q, double *x)
         }
     }
 }
+
+/* ------------------------------------------------------------------------ */
+/* Seeded synthetic workloads.  The reference has no generator of its own (it */
+/* reads SuiteSparse files, README.md:10, and fills B from a time(0)-seeded   */
+/* rand(), helper.h:66-76).  These restate, step for step, the library's      */
+/* generators (libdaspmm daspmm_gen_*) so that the benchmark's reference arm  */
+/* builds the same inputs without loading the product library; a CPU test     */
+/* checks them bit for bit against libdaspmm.                                 */
+/* ------------------------------------------------------------------------ */
+typedef struct { uint64_t s; } or_rng;
+
+static uint64_t rng_next(or_rng *g)
+{
+    /* splitmix64 (Steele, Lea, Flood 2014) */
+    uint64_t z = (g->s += 0x9e3779b97f4a7c15ULL);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+static double rng_uniform(or_rng *g) { return (double)(rng_next(g) >> 11) * 0x1.0p-53; }
+static float rng_unit24(or_rng *g) { return (float)(rng_next(g) >> 40) * 0x1.0p-24f; }
+static uint32_t rng_below(or_rng *g, uint32_t n)
+{
+    return (uint32_t)(((rng_next(g) >> 32) * (uint64_t)n) >> 32);
+}
+
+#define OR_DEG_STREAM 0x243f6a8885a308d3ULL
+#define OR_COL_STREAM 0x13198a2e03707344ULL
+#define OR_VAL_STREAM 0xa4093822299f31d0ULL
+
+static void gen_values(uint64_t seed, long long nnz, float *values)
+{
+    or_rng g = {seed ^ OR_VAL_STREAM};
+    for (long long p = 0; p < nnz; ++p) values[p] = rng_unit24(&g) * 2.0f - 1.0f;
+}
+
+static int cmp_int(const void *a, const void *b)
+{
+    const int x = *(const int *)a, y = *(const int *)b;
+    return (x > y) - (x < y);
+}
+
+/* Column draw for one row: 0 = uniform over nc, 1 = preferential attachment
+ * (an urn of every endpoint drawn so far, plus one entry per column). */
+typedef struct { int kind, nc; const int *urn; size_t urn_n; } or_draw;
+
+static int draw_col(or_rng *g, const or_draw *d)
+{
+    if (d->kind == 0) return (int)rng_below(g, (uint32_t)d->nc);
+    const uint32_t u = rng_below(g, (uint32_t)(d->urn_n + (size_t)d->nc));
+    return u < (uint32_t)d->nc ? (int)u : d->urn[u - (uint32_t)d->nc];
+}
+
+/* `deg` distinct columns for row r: up to 64 draws per column, then uniform
+ * redraws; stamp[c] == r marks a column already taken; sorted ascending. */
+static void distinct_row(int r, int deg, int nc, int *stamp, or_rng *g, const or_draw *d,
+                         int *out)
+{
+    for (int j = 0; j < deg; ++j) {
+        int col = -1;
+        for (int tries = 0; tries < 64; ++tries) {
+            const int c = draw_col(g, d);
+            if (stamp[c] != r) { col = c; break; }
+        }
+        while (col < 0) {
+            const int c = (int)rng_below(g, (uint32_t)nc);
+            if (stamp[c] != r) col = c;
+        }
+        stamp[col] = r;
+        out[j] = col;
+    }
+    qsort(out, (size_t)deg, sizeof(int), cmp_int);
+}
+
+int or_gen_uniform(int nr, int nc, int per_row, uint64_t seed, int *rowPtr, int *colIdx,
+                   float *values)
+{
+    if (nr < 0 || nc < 1 || per_row < 0 || per_row > nc || !rowPtr) return -1;
+    if ((long long)nr * per_row > 0x7fffffffLL) return -1;
+    for (int r = 0; r <= nr; ++r) rowPtr[r] = r * per_row;
+    if (!colIdx || !values) return 0;
+    or_rng g = {seed ^ OR_COL_STREAM};
+    int *stamp = (int *)malloc(sizeof(int) * (size_t)nc);
+    if (!stamp) return -1;
+    for (int c = 0; c < nc; ++c) stamp[c] = -1;
+    const or_draw d = {0, nc, NULL, 0};
+    for (int r = 0; r < nr; ++r)
+        distinct_row(r, per_row, nc, stamp, &g, &d, colIdx + (size_t)r * per_row);
+    free(stamp);
+    gen_values(seed, (long long)nr * per_row, values);
+    return 0;
+}
+
+int or_gen_powerlaw(int nr, int nc, double alpha, double shift, int dmin, int dmax,
+                    double mean_scale, uint64_t seed, int *rowPtr, int *colIdx,
+                    float *values, long long *nnz_out)
+{
+    if (nr < 0 || nc < 1 || dmin < 0 || dmax < dmin || !rowPtr || mean_scale <= 0) return -1;
+    if (dmax > nc) dmax = nc;
+    if (dmin > dmax) dmin = dmax;
+    /* out-degree p(k) ~ (k + shift)^-alpha on [dmin, dmax], drawn by
+     * inverting the normalised cumulative sum (first entry > u) */
+    const int nk = dmax - dmin + 1;
+    double *cdf = (double *)malloc(sizeof(double) * (size_t)nk);
+    if (!cdf) return -1;
+    double acc = 0;
+    for (int k = dmin; k <= dmax; ++k) {
+        acc += pow((double)k + shift, -alpha);
+        cdf[k - dmin] = acc;
+    }
+    for (int i = 0; i < nk; ++i) cdf[i] /= acc;
+    or_rng gd = {seed ^ OR_DEG_STREAM};
+    long long nnz = 0;
+    rowPtr[0] = 0;
+    for (int r = 0; r < nr; ++r) {
+        const double u = rng_uniform(&gd);
+        int lo = 0, hi = nk; /* first i with cdf[i] > u */
+        while (lo < hi) {
+            const int mid = lo + (hi - lo) / 2;
+            if (cdf[mid] > u) hi = mid; else lo = mid + 1;
+        }
+        int k = dmin + lo;
+        if (k > dmax) k = dmax;
+        if (mean_scale != 1.0) {
+            k = (int)lround(k * mean_scale);
+            if (k > dmax) k = dmax;
+            if (k < dmin) k = dmin;
+        }
+        nnz += k;
+        if (nnz > 0x7fffffffLL) { free(cdf); return -1; }
+        rowPtr[r + 1] = (int)nnz;
+    }
+    free(cdf);
+    if (nnz_out) *nnz_out = nnz;
+    if (!colIdx || !values) return 0;
+    or_rng gc = {seed ^ OR_COL_STREAM};
+    int *urn = (int *)malloc(sizeof(int) * (size_t)(nnz > 0 ? nnz : 1));
+    int *stamp = (int *)malloc(sizeof(int) * (size_t)nc);
+    if (!urn || !stamp) { free(urn); free(stamp); return -1; }
+    for (int c = 0; c < nc; ++c) stamp[c] = -1;
+    size_t urn_n = 0;
+    for (int r = 0; r < nr; ++r) {
+        const int p0 = rowPtr[r], deg = rowPtr[r + 1] - p0;
+        const or_draw d = {1, nc, urn, urn_n};
+        distinct_row(r, deg, nc, stamp, &gc, &d, colIdx + p0);
+        for (int j = 0; j < deg; ++j) urn[urn_n++] = colIdx[p0 + j];
+    }
+    free(urn);
+    free(stamp);
+    gen_values(seed, nnz, values);
+    return 0;
+}
+
+void or_gen_dense(size_t n, uint64_t seed, float lo, float hi, float *out)
+{
+    or_rng g = {seed ^ OR_VAL_STREAM};
+    for (size_t i = 0; i < n; ++i) out[i] = lo + (hi - lo) * rng_unit24(&g);
+}

@@ -4,7 +4,8 @@
  * bit for bit.
  *
  * TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and the
- * cpu_baseline leg of bench.py may load this library, and only as the checker.
+ * cpu_baseline and reference legs of bench.py may load this library, and only
+ * as the checker (or, in the reference leg, to build that leg's inputs).
  * The shipped library (libdaspmm.so) never links or calls it.
  *
  * Every function cites the reference file:line it restates (paths relative to
@@ -120,6 +121,17 @@ float or_e4m3_to_f32(uint8_t v);
 void or_quantize(int fmt, size_t n, const float *x, void *q);
 void or_dequantize(int fmt, size_t n, const void *q, double *x);
 /* fmt ids: 0 = f32, 1 = bf16, 2 = f16, 3 = e4m3 (same as daspmm.h) */
+
+/* ---- Seeded synthetic workloads: restatements of libdaspmm's generators
+ * (daspmm_gen_uniform / _powerlaw / _dense), so that the benchmark's
+ * reference arm builds its inputs without the product library.  Same
+ * arguments and outputs; 0 on success, -1 on bad arguments. ---- */
+int or_gen_uniform(int nr, int nc, int per_row, uint64_t seed, int *rowPtr, int *colIdx,
+                   float *values);
+int or_gen_powerlaw(int nr, int nc, double alpha, double shift, int dmin, int dmax,
+                    double mean_scale, uint64_t seed, int *rowPtr, int *colIdx,
+                    float *values, long long *nnz_out);
+void or_gen_dense(size_t n, uint64_t seed, float lo, float hi, float *out);
 
 #ifdef __cplusplus
 }

@@ -49,6 +49,12 @@ def lib():
             "or_coo_ownership": (_I, [_I, _I, _VP, _I, _VP]),
             "or_quantize": (None, [_I, ctypes.c_size_t, _VP, _VP]),
             "or_dequantize": (None, [_I, ctypes.c_size_t, _VP, _VP]),
+            "or_gen_uniform": (_I, [_I, _I, _I, ctypes.c_uint64, _VP, _VP, _VP]),
+            "or_gen_powerlaw": (_I, [_I, _I, ctypes.c_double, ctypes.c_double, _I, _I,
+                                     ctypes.c_double, ctypes.c_uint64, _VP, _VP, _VP,
+                                     ctypes.POINTER(ctypes.c_longlong)]),
+            "or_gen_dense": (None, [ctypes.c_size_t, ctypes.c_uint64, ctypes.c_float,
+                                    ctypes.c_float, _VP]),
         }
         for n, (r, a) in sig.items():
             f = getattr(L, n)
@@ -194,6 +200,59 @@ def dequantize(fmt: int, q) -> np.ndarray:
     x = np.zeros(q.size, np.float64)
     lib().or_dequantize(fmt, q.size, _p(q), _p(x))
     return x
+
+
+# ---------------------------------------------------------------- workloads
+class HostCsr:
+    """A host CSR matrix built by the oracle's generators (int32 / float32)."""
+
+    def __init__(self, nr, nc, rowPtr, colIdx, values):
+        self.nr, self.nc = nr, nc
+        self.rowPtr, self.colIdx, self.values = rowPtr, colIdx, values
+
+    @property
+    def nnz(self) -> int:
+        return int(self.rowPtr[-1]) if self.nr > 0 else 0
+
+    def cols_touched(self) -> int:
+        return int(np.unique(self.colIdx).size) if self.nnz else 0
+
+
+def gen_uniform(nr: int, nc: int, per_row: int, seed: int = 0) -> HostCsr:
+    """Exactly per_row distinct uniform columns per row, values U(-1,1)
+    (restates libdaspmm's daspmm_gen_uniform)."""
+    rp = np.zeros(nr + 1, np.int32)
+    n = nr * per_row
+    ci = np.zeros(max(1, n), np.int32)
+    va = np.zeros(max(1, n), np.float32)
+    if lib().or_gen_uniform(nr, nc, per_row, seed, _p(rp), _p(ci), _p(va)) != 0:
+        raise ValueError("gen_uniform: bad arguments")
+    return HostCsr(nr, nc, rp, ci[:n].copy(), va[:n].copy())
+
+
+def gen_powerlaw(n: int, alpha: float = 2.1, shift: float = 0.16, dmin: int = 1,
+                 dmax: int = 4096, seed: int = 0, mean_scale: float = 1.0,
+                 nc: int | None = None) -> HostCsr:
+    """Power-law out-degrees (k + shift)^-alpha on [dmin, dmax], preferential-
+    attachment columns, values U(-1,1) (restates daspmm_gen_powerlaw)."""
+    nc = n if nc is None else nc
+    rp = np.zeros(n + 1, np.int32)
+    nnz = ctypes.c_longlong(0)
+    if lib().or_gen_powerlaw(n, nc, alpha, shift, dmin, dmax, mean_scale, seed, _p(rp), None,
+                             None, ctypes.byref(nnz)) != 0:
+        raise ValueError("gen_powerlaw: bad arguments")
+    ci = np.zeros(max(1, nnz.value), np.int32)
+    va = np.zeros(max(1, nnz.value), np.float32)
+    lib().or_gen_powerlaw(n, nc, alpha, shift, dmin, dmax, mean_scale, seed, _p(rp), _p(ci),
+                          _p(va), ctypes.byref(nnz))
+    return HostCsr(n, nc, rp, ci[:nnz.value].copy(), va[:nnz.value].copy())
+
+
+def gen_dense(n: int, seed: int = 1, lo: float = -1.0, hi: float = 1.0) -> np.ndarray:
+    """n floats U(lo, hi) on a 2^-24 grid (restates daspmm_gen_dense)."""
+    out = np.empty(max(1, n), np.float32)
+    lib().or_gen_dense(n, seed, lo, hi, _p(out))
+    return out[:n]
 
 
 # ---------------------------------------------------------------- tolerances
