@@ -354,6 +354,9 @@ def run_ours(args):
             cpu = {"value": round(2.0 * nnz_s * NV / (ms_cpu * 1e-3) / 1e9, 3), "unit": UNIT,
                    "cores": cores, "kind": kind,
                    "sample": f"full matrix ({nnz_s} nnz, N=128), median of 3 passes, 1 thread"}
+        refk, cus = (None, None) if (args.no_refk or world > 1) else \
+            run_reference_kernels(A, dA, Bt, dev, ms_step)
+        variants = None if (args.no_variants or world > 1) else run_variants(D, A, dA, Bt, dev, peak)
         mixed = None if args.no_mixed else run_mixed(D, A, dA, B, dev, K, peak)
         if mixed is not None and world == 1:
             mixed["random_1m_deg8"] = run_mixed_random(D, dev, peak)
@@ -382,6 +385,7 @@ def run_ours(args):
                          "peak_source": peak_src},
             "step_hbm_gbs": round(abytes / (ms_step * 1e-3) / 1e9, 1),
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": int(launches),
+            "reference_kernels": refk, "cusparse": cus, "variants": variants,
             "mixed": mixed, "batched": batched, "serving": serving,
         }
     if pg:
@@ -390,6 +394,95 @@ def run_ours(args):
     if line is not None:
         print(json.dumps(line), flush=True)
     return 0
+
+
+REF_VARIANTS = [  # run.sh:29 column order: alg (spmvspmm.h:5-10) x layout
+    ("SR_RB_RM", 0, 0), ("PR_RB_RM", 1, 0), ("SR_EB_RM", 2, 0), ("PR_EB_RM", 3, 0),
+    ("SR_RB_CM", 0, 1), ("PR_RB_CM", 1, 1), ("SR_EB_CM", 2, 1), ("PR_EB_CM", 3, 1)]
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def run_reference_kernels(A, dA, Bt, dev, ours_ms, warmup=3, reps=20):
+    """The reference's own GPU kernels (cudaSpmm<256,32>, spmvspmm.h:53-199, in
+    oracle/_ref/libref.so, built from the unmodified reference) on the same
+    device matrix and B, timed by the reference's own loop
+    (SpmvSpmmProblem::benchmark, spmvspmm.h:220-243: CUDA events around
+    `reps` launches on stream 0), for the 8 variants of run.sh:29; and
+    cuSPARSE through the reference's helper (cusparse_helper.h:385-434) with
+    the algorithms of spmvspmm_benchmark.cu:309-312.  Comparison lines: they
+    run after the timed region."""
+    import torch
+    from oracle import oracle as O
+    if not O.ref_available():
+        return {"unavailable": "oracle/_ref/libref.so not built"}, None
+    R = O.ref()
+    C = torch.zeros(A.nr * NV, device=dev)
+    flop = 2.0 * A.nnz * NV
+    ptrs = [_ptr(dA.rowPtr), _ptr(dA.rowIdx), _ptr(dA.colIdx), _ptr(dA.values), _ptr(Bt), _ptr(C)]
+    kern = {}
+    for name, alg, layout in REF_VARIANTS:
+        ms = R.ref_cuda_bench(alg, layout, A.nr, A.nc, A.nnz, NV, *ptrs, warmup, reps)
+        torch.cuda.synchronize(dev)
+        kern[name] = {"us": round(ms * 1e3, 2), "gflops": round(flop / (ms * 1e-3) / 1e9, 1)}
+    best = min(kern, key=lambda k: kern[k]["us"])
+    kern["best"] = best
+    kern["daspmm_speedup_vs_best"] = round(kern[best]["us"] / (ours_ms * 1e3), 3)
+    kern["timing"] = (f"SpmvSpmmProblem::benchmark: {warmup} warm-up + {reps} timed launches, "
+                      "CUDA events on stream 0, ms per launch")
+    cus = {}
+    for name, fmt, layout, alg in (("csr_row_default", 0, 0, 0), ("csr_row_alg2", 0, 0, 6),
+                                   ("coo_row_default", 1, 0, 0), ("coo_row_alg4", 1, 0, 5),
+                                   ("csr_col_default", 0, 1, 0), ("csr_col_alg1", 0, 1, 4)):
+        ms = R.ref_cusparse_bench(fmt, layout, A.nr, A.nc, A.nnz, NV, *ptrs, alg, warmup, reps)
+        torch.cuda.synchronize(dev)
+        cus[name] = {"us": round(ms * 1e3, 2), "gflops": round(flop / (ms * 1e-3) / 1e9, 1)}
+    bestc = min(cus, key=lambda k: cus[k]["us"])
+    cus["best"] = bestc
+    cus["daspmm_speedup_vs_best"] = round(cus[bestc]["us"] / (ours_ms * 1e3), 3)
+    del C
+    return kern, cus
+
+
+def run_variants(D, A, dA, Bt, dev, peak, K=20):
+    """This library's own design space on the same matrix and N: every
+    algorithm (RB/EB x SR/PR; the balanced CSR split with each of its
+    pipelines) in both layouts at its default lanes / coarsening, K calls back
+    to back between CUDA events.  Bytes model as the roofline's."""
+    import torch
+    C = torch.zeros(A.nr * NV, device=dev)
+    abytes = algorithmic_bytes(A, NV)
+    flop = 2.0 * A.nnz * NV
+    out = {}
+    points = [("CSR_SCALAR", 0, 0, 0), ("CSR_VECTOR", 1, 0, 0), ("COO_SCALAR", 2, 0, 0),
+              ("COO_VECTOR", 3, 0, 0), ("CSR_BALANCED pipe1 register gather", 4, 0, 1),
+              ("CSR_BALANCED pipe2 TMA ring", 4, 0, 2),
+              ("CSR_BALANCED pipe3 cp.async ring", 4, 0, 3),
+              ("CSR_BALANCED pipe4 window kernel (default)", 4, 0, 4),
+              ("CSR_SCALAR", 0, 1, 0), ("CSR_VECTOR", 1, 1, 0), ("COO_SCALAR", 2, 1, 0),
+              ("COO_VECTOR", 3, 1, 0), ("CSR_BALANCED pipe1 direct gather", 4, 1, 1),
+              ("CSR_BALANCED pipe5 via row-major (default)", 4, 1, 5)]
+    for name, alg, layout, pipe in points:
+        cfg = D.Config(alg=alg, pipe=pipe)
+        run = lambda: D.spmm(alg, layout, dA, Bt, C, nv=NV, cfg=cfg)
+        for _ in range(3):
+            run()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(K):
+            run()
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / K
+        key = f"{name} {'RM' if layout == 0 else 'CM'}"
+        out[key] = {"us": round(ms * 1e3, 2), "gflops": round(flop / (ms * 1e-3) / 1e9, 1),
+                    "gbs": round(abytes / (ms * 1e-3) / 1e9, 1),
+                    "frac": round(abytes / (ms * 1e-3) / 1e9 / peak, 4)}
+    del C
+    return out
 
 
 def run_mixed(D, A, dA, B, dev, steps, peak):
@@ -697,6 +790,10 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-refk", action="store_true",
+                    help="skip the reference's own kernels and cuSPARSE comparison lines")
+    ap.add_argument("--no-variants", action="store_true",
+                    help="skip the per-variant timing of this library's design space")
     ap.add_argument("--serve-seconds", type=float, default=1.0)
     args = ap.parse_args()
     if args.impl == "reference":

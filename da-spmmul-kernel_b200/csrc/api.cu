@@ -207,9 +207,10 @@ daspmm_status resolve(const daspmm_config *cfg, int layout, int nr, int nc, int 
                 if (r.pipe == 4) {
                     // measured on the 262k power-law and 1M random matrices: one
                     // 128-column tile runs best at 96 nonzeros per chunk (FP32
-                    // 93.3 -> 88.6 us on the power-law matrix), wider products
-                    // (several tiles in flight) at 128
-                    r.chunk = nv == 128 ? 96 : 128;
+                    // 93.3 -> 88.6 us on the power-law matrix), one 64-column
+                    // tile at 64 (56.8 -> 53.8 us), wider products (several
+                    // tiles in flight) at 128
+                    r.chunk = nv == 128 ? 96 : (nv == 64 ? 64 : 128);
                 } else {
                     // rings: one wave of chunks over the resident warps (12 per SM)
                     const long long slots = (long long)device_sms() * 12;
@@ -683,6 +684,35 @@ daspmm_status daspmm_coo_to_csr(int nr, int nnz, const int *rowIdx, int *rowPtr,
 }
 
 long long daspmm_launch_count(void) { return g_launches.load(); }
+
+// The bounded mbarrier wait of the ring kernels, run on its own: one thread
+// arms a barrier and waits on it with mbar_wait.  With `expire`, the barrier
+// expects 16 transaction bytes that no copy will ever deliver (nothing is
+// issued, so nothing is in flight), so the wait runs out after `polls` polls
+// and sets the device error word; otherwise the thread's own arrival
+// completes the phase.  out[0] = 1 if the wait returned success, else 0.
+static __global__ void k_wait_probe(int polls, int expire, int *out)
+{
+    __shared__ __align__(8) unsigned long long bar;
+    if (threadIdx.x != 0) return;
+    const uint32_t b = smem_addr(&bar);
+    mbar_init(b, 1);
+    mbar_init_fence();
+    if (expire) mbar_arrive_expect_tx(b, 16);
+    else mbar_arrive(b);
+    const bool ok = mbar_wait(b, 0, polls);
+    mbar_inval(b);
+    out[0] = ok ? 1 : 0;
+}
+
+daspmm_status daspmm_wait_probe(int polls, int expire, int *out, void *stream)
+{
+    if (polls < 1 || !out) return DASPMM_ERR_INVALID;
+    k_wait_probe<<<1, 32, 0, (cudaStream_t)stream>>>(polls, expire ? 1 : 0, out);
+    count_launches(1);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? DASPMM_OK : cuda_fail(e);
+}
 
 daspmm_status daspmm_device_error(void)
 {

@@ -325,9 +325,10 @@ __global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_fast(const KArgs 
     // A chunk's last window is padded with column 0, value 0: that adds
     // nothing unless row 0 of B holds an Inf or NaN (0 * Inf = NaN).  Then
     // every chunk is handed to the walk kernel, which never pads (the same
-    // decision in every warp and column tile).
+    // decision in every warp and column tile).  Without nonzeros nothing is
+    // padded (and B may have no rows).
     bool pad_ok = true;
-    for (int k = lane; k < a.nv; k += 32) {
+    for (int k = lane; a.nnz > 0 && k < a.nv; k += 32) {
         float x[1];
         ld_b<TB, 1>(x, reinterpret_cast<const TB *>(a.B) + k);
         pad_ok &= isfinite(x[0]);
@@ -473,24 +474,24 @@ __device__ __forceinline__ void ld_cg_n(float (&r)[VL], const float *p)
     else ld_cg<VL>(r, p);
 }
 
-// piece_arrive for a 16-lane half of a warp (lanes of `hmask`, VL floats per
+// piece_arrive for a G-lane worker of a warp (lanes of `gmask`, VL floats per
 // lane at column `col`), beta == 0: the same counters, carries and order of
 // summation as piece_arrive, so the two combine pieces of one row freely.
 // Templated on the kernel's types so that every kernel has its own copy:
 // ptxas 12.9 crashes (at build time) on one copy shared by two kernels.
-template <int VL, typename TV, typename TB>
-static __device__ __noinline__ void piece_arrive_half(const int *__restrict__ rowPtr, int *cnt,
-                                               const float *slots, float *C, int ldc, int nv,
-                                               int chunk, int row, int col, int tiles, int tile,
-                                               unsigned hmask)
+template <int G, int VL, typename TV, typename TB>
+static __device__ __noinline__ void piece_arrive_grp(const int *__restrict__ rowPtr, int *cnt,
+                                                     const float *slots, float *C, int ldc,
+                                                     int nv, int chunk, int row, int col,
+                                                     int tiles, int tile, unsigned gmask)
 {
     const int rs = __ldg(rowPtr + row), re = __ldg(rowPtr + row + 1);
     const int c0 = first_chunk(rs, chunk), c1 = last_chunk(re, chunk);
     __threadfence();
-    __syncwarp(hmask);
+    __syncwarp(gmask);
     int last = 0;
-    if ((threadIdx.x & 15) == 0) last = atomicAdd(cnt + (size_t)c0 * tiles + tile, 1) == c1 - c0;
-    last = __shfl_sync(hmask, last, 0, 16);
+    if ((threadIdx.x & (G - 1)) == 0) last = atomicAdd(cnt + (size_t)c0 * tiles + tile, 1) == c1 - c0;
+    last = __shfl_sync(gmask, last, 0, G);
     if (!last) return;
     __threadfence();
     float tot[VL];
@@ -510,58 +511,67 @@ static __device__ __noinline__ void piece_arrive_half(const int *__restrict__ ro
     st_n<VL>(C + (size_t)row * ldc + col, tot);
 }
 
-#ifndef DASPMM_HALF
-#define DASPMM_HALF 1       // FP32 128-column tiles take the half-warp kernel
+#ifndef DASPMM_GRP
+#define DASPMM_GRP 1        // FP32 32/64/128-column tiles take the worker-group kernel
 #endif
-#ifndef DASPMM_HALF_U
-#define DASPMM_HALF_U 8     // nonzeros in flight per half-warp step
+#ifndef DASPMM_GRP_U
+#define DASPMM_GRP_U 8      // nonzeros in flight per worker step
 #endif
-#ifndef DASPMM_HALF_MINB
-#define DASPMM_HALF_MINB 2  // CTAs of 256 threads per SM: 16 warps, <= 128 registers
+#ifndef DASPMM_GRP_MINB
+#define DASPMM_GRP_MINB 2   // CTAs of 256 threads per SM: 16 warps, <= 128 registers
 #endif
 
-// k_bal_fast with a 16-lane worker: FP32, 128-column tiles, beta == 0, B and C
-// 32-byte aligned.  Each half of a warp takes one chunk of a pair (2p, 2p+1)
-// and covers a B row of 128 floats with 16 lanes x 32-byte loads, so one warp
-// instruction gathers two nonzeros -- half the instructions per nonzero of
-// the 32-lane form and twice the bytes in flight per warp.  The halves run in
-// step: the window loop runs to the longer chunk of the pair (balanced chunks
-// differ by a few nonzeros); a half past its chunk's end gathers padding
-// (column 0, value 0) and stores nothing.  Windows are 16 nonzeros (lane l of
-// a half ends row r + l), the rest is
-// k_bal_fast's: same chunks, carries, split-row combine and order of
-// summation, so results are bit-identical to it.
-template <int U, int VL = 8, typename TV = float, typename TB = float>
-__global__ void __launch_bounds__(256, DASPMM_HALF_MINB) k_bal_half(const KArgs a)
+// k_bal_fast with G-lane workers: FP32, column tiles of 8*G floats (G = 16:
+// 128, 8: 64, 4: 32), beta == 0, B and C 32-byte aligned.  Each worker (G
+// consecutive lanes) takes one chunk of a group (32/G consecutive chunks per
+// warp) and covers its tile of a B row with G lanes x 32-byte loads
+// (ld.global.nc.v8.f32), so one warp instruction gathers 32/G nonzeros -- 256
+// bytes per lane-load whatever the tile width.  The workers run in step: the
+// window loop runs to the longest chunk of the group (balanced chunks differ
+// by a few nonzeros); a worker past its chunk's end gathers padding (column
+// 0, value 0) and stores nothing.  Windows are G nonzeros (lane l of a
+// worker ends row r + l), gathered min(U, G) B rows at a time.  Everything
+// else is k_bal_fast's: same chunks, carries, split-row
+// combine and order of summation, so results are bit-identical to it.
+// Column tiles are blockIdx.y: the CTAs of tile 0 are dispatched first, so
+// with several tiles their B column slabs are gathered one after the other
+// (each slab a fraction of B in L2).
+template <int G, int U, typename TV = float, typename TB = float>
+__global__ void __launch_bounds__(256, DASPMM_GRP_MINB) k_bal_grp(const KArgs a)
 {
+    constexpr int VL = 8;              // floats per lane: one 32-byte load
+    constexpr int NW = 32 / G;         // workers per warp
+    constexpr int UU = U < G ? U : G;  // rows in flight per step (within one window)
+    constexpr unsigned GM = G == 32 ? 0xFFFFFFFFu : ((1u << G) - 1u);
     constexpr bool SCALED = std::is_same<TB, fp8>::value;
-    const int lane = threadIdx.x & 31, h = lane >> 4, hl = lane & 15;
-    const unsigned hmask = 0xFFFFu << (16 * h);
+    const int lane = threadIdx.x & 31, w = lane / G, gl = lane % G;
+    const unsigned gmask = GM << (G * w);
     const int tile = blockIdx.y, tiles = gridDim.y;
-    const int tb = tile * (16 * VL) + hl * VL;
+    const int tb = tile * (G * VL) + gl * VL;
     const TB *Bl = reinterpret_cast<const TB *>(a.B) + tb;
     const TV *Av = reinterpret_cast<const TV *>(a.vals);
-    float sc[VL];
-#pragma unroll
-    for (int e = 0; e < VL; ++e) sc[e] = SCALED ? __ldg(a.bscale + tb + e) : 1.0f;
     const uint64_t pol_once = policy_evict_first();
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    const long long npairs = ((long long)a.nchunks + 1) >> 1;
+    const long long ngroups = ((long long)a.nchunks + NW - 1) / NW;
 
     pdl_trigger();  // the list-mode walk may be scheduled; it waits for this grid
     pdl_wait();     // the boundaries from k_partition are complete
+    float sc[VL];   // read after the wait, like every input
+#pragma unroll
+    for (int e = 0; e < VL; ++e) sc[e] = SCALED ? __ldg(a.bscale + tb + e) : 1.0f;
     // padding (column 0, value 0) adds nothing unless row 0 of B holds an Inf
-    // or NaN; then every chunk is handed to the walk kernel (as in k_bal_fast)
+    // or NaN; then every chunk is handed to the walk kernel (as in k_bal_fast).
+    // Without nonzeros nothing is padded (and B may have no rows).
     bool pad_ok = true;
-    for (int k = lane; k < a.nv; k += 32) {
+    for (int k = lane; a.nnz > 0 && k < a.nv; k += 32) {
         float x[1];
         ld_b<TB, 1>(x, reinterpret_cast<const TB *>(a.B) + k);
         pad_ok &= isfinite(x[0]);
     }
     pad_ok = __all_sync(kFull, pad_ok);
-    long long pl = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    while (pl < npairs) {
-        const int c = (int)(2 * pl) + h;
+    long long gi = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    while (gi < ngroups) {
+        const int c = (int)(NW * gi) + w;
         const bool have = c < a.nchunks;
         int k0 = 0, k1 = 0, s1 = 0, r = 0, rstart = 0;
         if (have) {
@@ -573,73 +583,74 @@ __global__ void __launch_bounds__(256, DASPMM_HALF_MINB) k_bal_half(const KArgs 
             rstart = __ldg(a.rowPtr + r);
         }
         const int r0 = r;
-        // ends of rows r .. r+15; any empty row among [r, s1) hands the chunk on
-        int E = __ldg(a.rowPtr + min(r + 1 + hl, a.nr));
+        // ends of rows r .. r+G-1; any empty row among [r, s1) hands the chunk on
+        int E = __ldg(a.rowPtr + min(r + 1 + gl, a.nr));
         bool empty_row;
         {
-            int prev = __shfl_up_sync(kFull, E, 1, 16);
-            if (hl == 0) prev = rstart;
-            empty_row = (__ballot_sync(kFull, have && r + hl < s1 && E == prev) & hmask) != 0;
-            int last = __shfl_sync(kFull, E, 15, 16);
-            bool more = have && !empty_row && r + 16 < s1;
-            for (int rb = r + 16; __any_sync(kFull, more); rb += 16) {
+            int prev = __shfl_up_sync(kFull, E, 1, G);
+            if (gl == 0) prev = rstart;
+            empty_row = (__ballot_sync(kFull, have && r + gl < s1 && E == prev) & gmask) != 0;
+            int last = __shfl_sync(kFull, E, G - 1, G);
+            bool more = have && !empty_row && r + G < s1;
+            for (int rb = r + G; __any_sync(kFull, more); rb += G) {
                 int e2 = 0;
-                if (more) e2 = __ldg(a.rowPtr + min(rb + 1 + hl, a.nr));
-                int p2 = __shfl_up_sync(kFull, e2, 1, 16);
-                if (hl == 0) p2 = last;
-                const unsigned b2 = __ballot_sync(kFull, more && rb + hl < s1 && e2 == p2);
-                if (more) empty_row = (b2 & hmask) != 0;
-                last = __shfl_sync(kFull, e2, 15, 16);
-                more = more && !empty_row && rb + 16 < s1;
+                if (more) e2 = __ldg(a.rowPtr + min(rb + 1 + gl, a.nr));
+                int p2 = __shfl_up_sync(kFull, e2, 1, G);
+                if (gl == 0) p2 = last;
+                const unsigned b2 = __ballot_sync(kFull, more && rb + gl < s1 && e2 == p2);
+                if (more) empty_row = (b2 & gmask) != 0;
+                last = __shfl_sync(kFull, e2, G - 1, G);
+                more = more && !empty_row && rb + G < s1;
             }
         }
         const bool skip = !have || empty_row || !pad_ok;
-        if (have && (empty_row || !pad_ok) && tile == 0 && hl == 0)
+        if (have && (empty_row || !pad_ok) && tile == 0 && gl == 0)
             a.list[1 + atomicAdd(a.list, 1)] = c;  // every tile
         const int kb = skip ? 0 : k0, ke = skip ? 0 : k1;
-        int nwin = (ke - kb + 15) >> 4;
-        nwin = max(nwin, __shfl_xor_sync(kFull, nwin, 16));
+        int nwin = (ke - kb + G - 1) / G;
+#pragma unroll
+        for (int o = G; o < 32; o <<= 1) nwin = max(nwin, __shfl_xor_sync(kFull, nwin, o));
         bool cont = !skip && k0 > rstart;
         const bool head_piece = cont;
         float acc[VL];
 #pragma unroll
         for (int e = 0; e < VL; ++e) acc[e] = 0.0f;
         auto load_win = [&](int wb, int &col, float &val) {
-            const bool ok = wb + hl < ke;
-            col = ok ? ld_hint_s32(a.colIdx + wb + hl, pol_once) : 0;
-            val = ok ? ld_val<TV>(Av + wb + hl, pol_once) : 0.0f;
+            const bool ok = wb + gl < ke;
+            col = ok ? ld_hint_s32(a.colIdx + wb + gl, pol_once) : 0;
+            val = ok ? ld_val<TV>(Av + wb + gl, pol_once) : 0.0f;
         };
         int ccur, cnext;
         float vcur, vnext;
         int wb = kb;
         load_win(wb, ccur, vcur);
-        for (int w = 0; w < nwin; ++w, wb += 16) {
-            load_win(wb + 16, cnext, vnext);
-            const int cnt = ke - wb;  // nonzeros of this half left (<= 0: idle)
+        for (int wi = 0; wi < nwin; ++wi, wb += G) {
+            load_win(wb + G, cnext, vnext);
+            const int cnt = ke - wb;  // nonzeros of this worker left (<= 0: idle)
             const int pos = E - 1 - wb;
-            const bool in = r + 1 + hl <= a.nr && pos >= 0 && pos < min(cnt, 16);
-            const unsigned e32 = __reduce_or_sync(kFull, in ? (1u << (pos + 16 * h)) : 0u);
-            const unsigned ends = (e32 >> (16 * h)) & 0xFFFFu;
+            const bool in = r + 1 + gl <= a.nr && pos >= 0 && pos < min(cnt, G);
+            const unsigned e32 = __reduce_or_sync(kFull, in ? (1u << (pos + G * w)) : 0u);
+            const unsigned ends = (e32 >> (G * w)) & GM;
             // the next window's row ends load while this one is summed
-            E = __ldg(a.rowPtr + min(r + __popc(ends) + 1 + hl, a.nr));
+            E = __ldg(a.rowPtr + min(r + __popc(ends) + 1 + gl, a.nr));
             float *cdst = cont ? slot_ptr(a, c, 0, tb) : a.C + (size_t)r * a.ldc + tb;
 #pragma unroll
-            for (int g = 0; g < 16 / U; ++g) {
-                int cc[U];
-                float vv[U];
+            for (int g = 0; g < G / UU; ++g) {
+                int cc[UU];
+                float vv[UU];
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    cc[u] = __shfl_sync(kFull, ccur, g * U + u, 16);
-                    vv[u] = __shfl_sync(kFull, vcur, g * U + u, 16);
+                for (int u = 0; u < UU; ++u) {
+                    cc[u] = __shfl_sync(kFull, ccur, g * UU + u, G);
+                    vv[u] = __shfl_sync(kFull, vcur, g * UU + u, G);
                 }
-                float b[U][VL];
+                float b[UU][VL];
 #pragma unroll
-                for (int u = 0; u < U; ++u) ld_b<TB, VL>(b[u], Bl + (size_t)cc[u] * a.ldb);
+                for (int u = 0; u < UU; ++u) ld_b<TB, VL>(b[u], Bl + (size_t)cc[u] * a.ldb);
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
+                for (int u = 0; u < UU; ++u) {
 #pragma unroll
                     for (int e = 0; e < VL; ++e) acc[e] = fmaf(vv[u], b[u][e], acc[e]);
-                    if ((ends >> (g * U + u)) & 1u) {
+                    if ((ends >> (g * UU + u)) & 1u) {
                         if constexpr (SCALED) {
 #pragma unroll
                             for (int e = 0; e < VL; ++e) acc[e] *= sc[e];
@@ -668,15 +679,15 @@ __global__ void __launch_bounds__(256, DASPMM_HALF_MINB) k_bal_half(const KArgs 
             st_n<VL>(slot_ptr(a, c, cont ? 0 : 1, tb), acc);
         }
         if (head_piece)
-            piece_arrive_half<VL, TV, TB>(a.rowPtr, a.cnt, a.slots, a.C, a.ldc, a.nv, a.chunk, r0, tb, tiles,
-                              tile, hmask);
+            piece_arrive_grp<G, VL, TV, TB>(a.rowPtr, a.cnt, a.slots, a.C, a.ldc, a.nv, a.chunk,
+                                            r0, tb, tiles, tile, gmask);
         if (tail_piece)
-            piece_arrive_half<VL, TV, TB>(a.rowPtr, a.cnt, a.slots, a.C, a.ldc, a.nv, a.chunk, s1, tb, tiles,
-                              tile, hmask);
+            piece_arrive_grp<G, VL, TV, TB>(a.rowPtr, a.cnt, a.slots, a.C, a.ldc, a.nv, a.chunk,
+                                            s1, tb, tiles, tile, gmask);
         __syncwarp();
         unsigned int nx = 0;
         if (lane == 0) nx = atomicAdd(a.head + tile, 1u);
-        pl = nwarps + (long long)__shfl_sync(kFull, nx, 0);
+        gi = nwarps + (long long)__shfl_sync(kFull, nx, 0);
     }
 }
 
@@ -711,25 +722,29 @@ inline void launch_lean(const Resolved &r, KArgs a, cudaStream_t st)
         1, std::min<long long>(((long long)a.nchunks + 7) / 8, resident));
     if (!K && a.beta == 0.0f) {
         a.list_mode = 0;
-        // the half-warp kernel: HV = W / 16 elements of B per lane (one
-        // HV * sizeof(TB) byte load), HV * 4-byte stores of C and carries
-        constexpr int HV = W / 16;
-        const bool aligned_h =
-            (reinterpret_cast<uintptr_t>(a.B) % (HV * sizeof(TB))) == 0 &&
-            ((reinterpret_cast<uintptr_t>(a.C) | reinterpret_cast<uintptr_t>(a.slots)) %
-             (HV * 4)) == 0 &&
-            a.ldb % HV == 0 && a.ldc % HV == 0 && a.nv % W == 0;
+        // the worker-group kernel: G = W / 8 lanes per chunk, 32-byte loads of
+        // B, 32-byte stores of C and carries
+        constexpr int G = W / 8;
+        const bool aligned_g =
+            (reinterpret_cast<uintptr_t>(a.B) % 32) == 0 &&
+            ((reinterpret_cast<uintptr_t>(a.C) | reinterpret_cast<uintptr_t>(a.slots)) % 32) ==
+                0 &&
+            a.ldb % 8 == 0 && a.ldc % 8 == 0 && a.nv % W == 0;
         constexpr bool f32 = std::is_same<TV, float>::value && std::is_same<TB, float>::value;
-        // measured: the half-warp form wins for FP32 storage and 128-column
-        // tiles only (BF16 / E4M3 B: 16 / 8-byte lane loads; 64-column tiles
-        // (k_bal_half<U, 4>): 59.5 against 58.8 us at N = 64 -- k_bal_fast)
-        if (W == 128 && f32 && DASPMM_HALF && aligned_h) {
-            const long long pairs = ((long long)a.nchunks + 1) / 2;
-            const unsigned gh = (unsigned)std::max<long long>(
-                1, std::min<long long>((pairs + 7) / 8,
-                                       (long long)device_sms() * DASPMM_HALF_MINB));
-            if constexpr (f32 && W == 128)
-                launch_pdl(k_bal_half<DASPMM_HALF_U, HV>, dim3(gh, r.tiles), st, a);
+        // measured on the 262k power-law matrix: the group form wins for FP32
+        // storage and 128- or 64-column tiles (N = 128: 84 against 113 us,
+        // N = 64: 54 against 61 us); for 32-column tiles (G = 4) the 32-lane
+        // kernel is as fast or faster (41 against 42 us at N = 32).  BF16 /
+        // E4M3 B (16- / 8-byte lane loads in the half-warp form) ran slower
+        // than k_bal_fast.
+        if (f32 && W >= 64 && DASPMM_GRP && aligned_g) {
+            constexpr int NW = 32 / G;
+            const long long groups = ((long long)a.nchunks + NW - 1) / NW;
+            const unsigned gg = (unsigned)std::max<long long>(
+                1, std::min<long long>((groups + 7) / 8,
+                                       (long long)device_sms() * DASPMM_GRP_MINB));
+            if constexpr (f32 && W >= 64)
+                launch_pdl(k_bal_grp<G, DASPMM_GRP_U>, dim3(gg, r.tiles), st, a);
         } else if constexpr (W == 128) {
             launch_pdl(k_bal_fast<W, DASPMM_LEAN_U, TV, TB>, dim3(gx, r.tiles), st, a);
         } else {  // one queue of (tile, chunk) items

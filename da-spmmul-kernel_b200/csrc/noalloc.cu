@@ -12,6 +12,7 @@
 // the process exits.
 #include "internal.h"
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -23,10 +24,49 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[DASPMM_NOALLOC_
 
 constexpr int kMaxDevices = 128;
 std::mutex g_mu;
-void *g_addr[kMaxDevices] = {};
+// Per device: the array's device address and the id of the context it was
+// looked up in.  A device reset (cudaDeviceReset) ends that context; the next
+// call on the device sees a new context id and looks the address up again.
+struct Entry {
+    unsigned long long ctx;
+    void *addr;
+};
+Entry g_addr[kMaxDevices] = {};
+
+using CtxGetCurrent = CUresult (*)(CUcontext *);
+using CtxGetId = CUresult (*)(CUcontext, unsigned long long *);
+
+// The id of the current device's current context (0 when it cannot be read;
+// then the address is looked up on every call).  The two driver functions are
+// reached through the runtime, so the library does not link libcuda itself.
+unsigned long long current_context_id()
+{
+    static CtxGetCurrent get_current = nullptr;
+    static CtxGetId get_id = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        void *f1 = nullptr, *f2 = nullptr;
+        cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = q1;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) ==
+                cudaSuccess &&
+            q1 == cudaDriverEntryPointSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) == cudaSuccess &&
+            q2 == cudaDriverEntryPointSuccess) {
+            get_current = reinterpret_cast<CtxGetCurrent>(f1);
+            get_id = reinterpret_cast<CtxGetId>(f2);
+        }
+        tried = true;
+    }
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || get_current(&ctx) != CUDA_SUCCESS || !ctx ||
+        get_id(ctx, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
 
 // The device address of g_noalloc_scratch on the current device.  Looked up
-// once per device (the first call on that device), with the device current.
+// with the device current, on the first call in each context of the device.
 daspmm_status scratch_address(void **out)
 {
     int dev = 0;
@@ -34,13 +74,15 @@ daspmm_status scratch_address(void **out)
     if (e != cudaSuccess) return daspmm::cuda_fail(e);
     if (dev < 0 || dev >= kMaxDevices) return DASPMM_ERR_UNSUPPORTED;
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_addr[dev]) {
+    const unsigned long long ctx = current_context_id();  // 0 before this thread's first runtime call
+    if (!g_addr[dev].addr || ctx == 0 || g_addr[dev].ctx != ctx) {
         void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);  // makes the context current
         if (e != cudaSuccess) return daspmm::cuda_fail(e);
-        g_addr[dev] = p;
+        g_addr[dev].addr = p;
+        g_addr[dev].ctx = current_context_id();
     }
-    *out = g_addr[dev];
+    *out = g_addr[dev].addr;
     return DASPMM_OK;
 }
 

@@ -56,13 +56,23 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity)
 }
 
 // Wait for phase `parity` of the barrier; false (and the error word set) if
-// the bound expires.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+// the bound (`polls` polls) expires.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int polls = kWaitPolls)
 {
-    for (int i = 0; i < kWaitPolls; ++i)
+    for (int i = 0; i < polls; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     atomicExch(&g_device_error, kErrWaitExpired);
     return false;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_inval(uint32_t bar)
+{
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
 }
 
 // Programmatic dependent launch: a kernel launched with programmatic stream

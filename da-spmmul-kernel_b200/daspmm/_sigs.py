@@ -87,6 +87,7 @@ def apply(lib, Config):
         "daspmm_quantize": (_I, [_I, ctypes.c_size_t, _VP, _VP, _VP, _I, _VP]),
         "daspmm_e4m3_scales": (_I, [_I, _I, _VP, _VP, _VP]),
         "daspmm_device_error": (_I, []),
+        "daspmm_wait_probe": (_I, [_I, _I, _VP, _VP]),
         "daspmm_mtx_info": (_I, [ctypes.c_char_p, ctypes.POINTER(MtxHeader)]),
         "daspmm_mtx_read": (_I, [ctypes.c_char_p, _I, _LL, _VP, _VP, _VP, _VP,
                                  ctypes.POINTER(_I)]),

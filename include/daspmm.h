@@ -416,16 +416,21 @@ daspmm_status daspmm_spmm_host_async(const daspmm_config *cfg, int layout, int n
  * DASPMM_NOALLOC_MAX_BYTES inside the library, which every GPU that loads the
  * library keeps until the process exits.  Nothing is allocated, by this
  * library or any other.
- *   - Limit: daspmm_workspace_bytes() of the DASPMM_ALG_CSR_BALANCED default
- *     configuration (daspmm_default_config) must be <= DASPMM_NOALLOC_MAX_BYTES.
- *     That is about 8 * nchunks * nv bytes (two carry rows per chunk), with
- *     nchunks = ceil(nnz / chunk): chunk = 96 for nv = 128 and 128 for the
- *     other row-major nv that are multiples of 32 (32..128 otherwise).  So
- *     nv = 128 fits up to about 1.6 M nonzeros (the 262,144-row power-law
- *     matrix, 1.24 M, needs 13.4 MB), nv = 32 about 8 M.  Larger problems
+ *   - Limit: daspmm_workspace_bytes(cfg, layout, nr, nc, nnz, nv) must be
+ *     <= DASPMM_NOALLOC_MAX_BYTES, with cfg = {.alg = DASPMM_ALG_CSR_BALANCED}
+ *     for row-major and {.alg = DASPMM_ALG_CSR_BALANCED, .pipe = 1} for
+ *     column-major (this entry point gathers column-major B directly, since
+ *     the transposing path would need room for copies of B and C).  That is
+ *     about 8 * nchunks * nv bytes (two carry rows per chunk), with nchunks =
+ *     ceil(nnz / chunk): row-major chunk = 96 for nv = 128, 64 for nv = 64
+ *     and 128 for the other nv that are multiples of 32 (32..128 otherwise);
+ *     column-major chunk = 32.  So row-major nv = 128 fits up to about 1.6 M
+ *     nonzeros (the 262,144-row power-law matrix, 1.24 M, needs 13.4 MB),
+ *     nv = 32 about 8 M; column-major nv = 16 about 4 M.  Larger problems
  *     return DASPMM_ERR_WORKSPACE before any device work.
- *   - The first call on each device looks up the array's device address with
- *     that device current; make that first call before any stream capture.
+ *   - The first call on each device (and the first after a cudaDeviceReset
+ *     of it) looks up the array's device address with that device current;
+ *     make that call before any stream capture.
  *   - All calls on a device share the one array.  Calls that overlap on the
  *     GPU (different streams, or different host threads, without ordering
  *     between them) race on it; order them.  The array keeps the last call's
@@ -442,6 +447,15 @@ daspmm_status daspmm_spmm_noalloc(int layout, int nr, int nc, int nnz, int nv,
  * DASPMM_ERR_TIMEOUT if a kernel's bounded wait expired since the last call
  * (that kernel stopped early and its output is incomplete). */
 daspmm_status daspmm_device_error(void);
+
+/* No counterpart in the reference.  Runs the bounded shared-memory barrier
+ * wait the ring kernels (pipes 2 and 3) use, alone, in one thread of one CTA:
+ * with `expire` != 0 the barrier expects bytes that nothing delivers (no copy
+ * is issued), so the wait gives up after `polls` polls, sets the device error
+ * word (read by daspmm_device_error) and the kernel returns; with expire == 0
+ * the wait succeeds at once.  Writes out[0] (device int) = 1 when the wait
+ * succeeded, 0 when it expired.  Asynchronous on `stream`. */
+daspmm_status daspmm_wait_probe(int polls, int expire, int *out, void *stream);
 
 /* Number of kernels this library has launched in this process. */
 long long daspmm_launch_count(void);

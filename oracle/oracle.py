@@ -297,6 +297,68 @@ def rel_err(c, c64, absc) -> float:
     return float((d / scale).max()) if d.size else 0.0
 
 
+def row_slice(rowPtr, colIdx, values, r0: int, r1: int):
+    """Rows [r0, r1) of a CSR matrix with their columns renumbered 0..m-1:
+    (rowPtr, colIdx, values, cols), where cols[j] is the original column of
+    new column j.  Lets the FP64 oracle check a row sample of a large product
+    with only the B rows that sample reads."""
+    rp = np.asarray(rowPtr)
+    p0, p1 = int(rp[r0]), int(rp[r1])
+    ci = np.asarray(colIdx[p0:p1])
+    cols = np.unique(ci)
+    return ((rp[r0:r1 + 1] - p0).astype(np.int32), np.searchsorted(cols, ci).astype(np.int32),
+            np.ascontiguousarray(values[p0:p1]), cols)
+
+
+ERR_FLOOR = 1e-3
+
+
+def error_stats(c, c64, absc) -> dict:
+    """Three statements of |c - c64| (c64 the FP64 oracle, absc = sum|a||b|
+    per element), over every element given:
+      norm_max      max|c - c64| / max absc            (max-norm relative)
+      cond_max      max |c - c64| / absc               (per element, relative to
+                                                        its own condition scale)
+      rel_floored   max |c - c64| / max(|c64|, ERR_FLOOR * max|c64|)
+                                                       (per element, relative to
+                                                        itself, small values floored)"""
+    c = np.asarray(c, np.float64).reshape(-1)
+    d = np.abs(c - c64)
+    m64 = float(np.max(np.abs(c64))) if c64.size else 0.0
+    den = np.maximum(np.abs(c64), ERR_FLOOR * m64) if m64 > 0 else np.ones_like(c64)
+    return {"norm_max": rel_err_max(c, c64, absc), "cond_max": rel_err(c, c64, absc),
+            "rel_floored": float((d / den).max()) if d.size else 0.0}
+
+
+def sample_rows(rowPtr, colIdx, nv: int, cap: int = 1 << 25) -> int:
+    """How many leading rows the FP64 oracle checks for an nv-column product:
+    all of them when the sample's output and its B rows stay under `cap`
+    elements each, else the largest power-of-two row count that does."""
+    rp = np.asarray(rowPtr)
+    nr = rp.size - 1
+    R = min(nr, max(1, cap // nv))
+    while R > 1:
+        ncols = np.unique(np.asarray(colIdx[: int(rp[R])])).size
+        if ncols * nv <= cap:
+            break
+        R //= 2
+    return R
+
+
+def mixed_errors(rp, ci, va32, va64, b32, b64, c, nv: int) -> dict:
+    """Error statements of a mixed-precision product on a row sample
+    (row_slice's compacted form): va32 / b32 the original FP32 values and B
+    rows, va64 / b64 their stored (quantized, scales applied) values as FP64,
+    c the device result for those rows.  `kernel` is the kernel's own
+    arithmetic (against FP64 of the stored inputs, per element relative to
+    its condition scale); `storage` is storage + arithmetic (against FP64 of
+    the FP32 inputs), as error_stats."""
+    nr, nc = rp.size - 1, b32.size // nv
+    cq, aq = spmm_f64d(0, nr, nc, rp, ci, va64, b64, nv)
+    c64, a64 = spmm_f64(0, nr, nc, rp, ci, va32, b32, nv)
+    return {"kernel": rel_err(c, cq, aq), "storage": error_stats(c, c64, a64)}
+
+
 def read_mtx(path: str, keep_diagonal: bool = False):
     """readMtx<float> (util/spmatrix.hpp:286-333) restated for small files,
     with makeSymmetric's value alignment fixed: returns (nr, nc, rows, cols,

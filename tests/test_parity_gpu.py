@@ -235,6 +235,24 @@ def test_edge_cases(cuda):
                     _check(A, layout, nv, B, C, what=f"edge nr={A.nr} nnz={A.nnz} {alg.name}")
 
 
+def test_no_columns_no_nonzeros(cuda):
+    """nr > 0 rows, no nonzeros and no columns: B has no rows, so nothing may
+    be read from it (the caller's pointer is valid but holds no row); C = 0
+    (beta = 0) or beta * C."""
+    import torch
+    A = D.Csr(6, 0, np.zeros(7, np.int32), np.zeros(0, np.int32), np.zeros(0, np.float32))
+    dA = _dev(A)
+    Bt = torch.zeros(1, device="cuda")   # a valid pointer to no B row
+    for nv in (1, 32, 128):
+        for layout in (0, 1):
+            for alg in ALGS:
+                for beta in (0.0, 0.5):
+                    C = torch.full((A.nr * nv,), 2.0, device="cuda")
+                    D.spmm(alg, layout, dA, Bt, C, beta=beta, nv=nv)
+                    torch.cuda.synchronize()
+                    assert torch.all(C == 2.0 * beta), f"{alg.name} layout {layout} nv {nv}"
+
+
 def test_partition_bit_exact(mats):
     for name in ("uniform", "powerlaw", "random", "hub"):
         A, dA = mats[name]
@@ -291,26 +309,37 @@ def test_full_size_configs(cuda):
         _check(A2, 0, nv, B, C, what=f"cfg2 {alg.name}")
 
 
-def test_half_warp_kernel_equals_32_lane_kernel(cuda):
-    """FP32 128-column tiles: with B and C 32-byte aligned the half-warp window
-    kernel runs, with both 16 bytes off that alignment the 32-lane one.  Same
-    chunks and order of summation: the products are bit-identical."""
+def test_group_kernel_equals_32_lane_kernel(cuda):
+    """FP32 row-major balanced CSR: with B and C 32-byte aligned the worker-
+    group window kernel runs (G = 16 / 8 / 4 lanes per chunk for 128 / 64 /
+    32-column tiles), with both 16 bytes off that alignment the 32-lane one.
+    Same chunks and order of summation: the products are bit-identical,
+    whatever the tile width."""
     import torch
     rng = np.random.default_rng(12)
     for A in (D.gen_powerlaw(20000, dmax=2000, seed=8), D.gen_random(5000, 4000, 5.0, seed=9)):
         dA = D.DeviceCsr(A)
-        for nv in (128, 256):
+        for nv in (32, 64, 96, 128, 256):
             B = rng.uniform(-1, 1, A.nc * nv).astype(np.float32)
             Ba = torch.from_numpy(B).cuda()
-            Ca = torch.empty(A.nr * nv, device="cuda")
             Bbuf = torch.zeros(A.nc * nv + 8, device="cuda")
             Cbuf = torch.zeros(A.nr * nv + 8, device="cuda")
             Bo, Co = Bbuf[4:4 + A.nc * nv], Cbuf[4:4 + A.nr * nv]
-            assert Ba.data_ptr() % 32 == 0 and Ca.data_ptr() % 32 == 0
+            assert Ba.data_ptr() % 32 == 0
             assert Bo.data_ptr() % 32 == 16 and Co.data_ptr() % 32 == 16
             Bo.copy_(Ba)
-            D.spmm(D.Alg.CSR_BALANCED, D.Layout.ROW_MAJOR, dA, Ba, Ca, nv=nv)
-            D.spmm(D.Alg.CSR_BALANCED, D.Layout.ROW_MAJOR, dA, Bo, Co, nv=nv)
-            torch.cuda.synchronize()
-            assert torch.equal(Ca, Co), f"nr={A.nr} nv={nv}: the two window kernels differ"
-            _check(A, 0, nv, B, Ca.cpu().numpy(), what=f"half-warp nv={nv}")
+            ref = None
+            for lanes in (0, 32, 16, 8):   # library tile width, then 128 / 64 / 32 columns
+                if lanes and nv % (4 * lanes):
+                    continue
+                cfg = D.Config(alg=int(D.Alg.CSR_BALANCED), lanes_col=lanes, chunk=96)
+                Ca = torch.full((A.nr * nv,), float("nan"), device="cuda")
+                D.spmm(D.Alg.CSR_BALANCED, D.Layout.ROW_MAJOR, dA, Ba, Ca, nv=nv, cfg=cfg)
+                if ref is None:
+                    D.spmm(D.Alg.CSR_BALANCED, D.Layout.ROW_MAJOR, dA, Bo, Co, nv=nv, cfg=cfg)
+                    torch.cuda.synchronize()
+                    ref = Co.clone()
+                    _check(A, 0, nv, B, ref.cpu().numpy(), what=f"32-lane nv={nv}")
+                torch.cuda.synchronize()
+                assert torch.equal(Ca, ref), \
+                    f"nr={A.nr} nv={nv} lanes_col={lanes}: the window kernels differ"

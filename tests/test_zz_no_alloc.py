@@ -104,3 +104,27 @@ def test_too_large_is_refused_before_device_work(cuda):
                     0.0, None)
     assert st == 5   # DASPMM_ERR_WORKSPACE
     torch.cuda.synchronize()
+
+
+def test_column_major_limit(cuda):
+    """Column-major calls gather B directly (no room for copies of B and C), so
+    their limit is the workspace of {CSR_BALANCED, pipe 1}: the largest nv
+    under the limit runs and matches daspmm_spmm, the next one is refused."""
+    import torch
+    A = D.gen_random(200000, 200000, 8.0, seed=4)
+    dA = D.DeviceCsr(A)
+    cfg = D.Config(alg=int(D.Alg.CSR_BALANCED), pipe=1)
+    ws = lambda nv: D.workspace_bytes(cfg, 1, A.nr, A.nc, A.nnz, nv)
+    fit = max(nv for nv in range(1, 200) if ws(nv) <= (16 << 20))
+    assert ws(fit + 1) > (16 << 20)
+    rng = np.random.default_rng(5)
+    B = rng.uniform(-1, 1, A.nc * fit).astype(np.float32)
+    for _ in range(2):
+        Cn, Ce = _both(A, dA, 1, fit, B)
+        _agree(A, 1, fit, B, Cn, Ce)
+    Bt = torch.zeros(A.nc * (fit + 1), device="cuda")
+    C = torch.zeros(A.nr * (fit + 1), device="cuda")
+    st = _noalloc()(1, A.nr, A.nc, A.nnz, fit + 1, _p(dA.rowPtr), _p(dA.colIdx),
+                    _p(dA.values), _p(Bt), _p(C), 0.0, None)
+    assert st == 5   # DASPMM_ERR_WORKSPACE
+    torch.cuda.synchronize()
