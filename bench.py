@@ -43,15 +43,20 @@ FALLBACK_HBM_GBS = 6650.0
 WORKLOAD = "FP32 CSR SpMM, power-law graph 262144x262144 (seed 0), B 262144x128 row-major"
 
 
-def bench_config(nr: int, nnz: int, world: int) -> dict:
+def bench_config(nr: int, nnz: int, world: int, scaling: str = "weak") -> dict:
     """The workload as both arms print it (identical keys and values)."""
+    if world > 1 and scaling == "strong":
+        par = f"one matrix cut into {world} row shards (balanced by nonzeros + rows), B replicated"
+    elif world > 1:
+        par = f"row shards x{world} (one 262144-row block per rank), B replicated, no collective"
+    else:
+        par = "single GPU"
     return {"workload": WORKLOAD, "nr": nr, "nnz": nnz, "nv": NV,
             "matrix": "out-degree (k+0.16)^-2.1 on [1,4096], preferential-attachment columns, "
                       "values U(-1,1); B U(-1,1) seed 1",
             "l2": "inputs larger than L2 (B 134 MB read + C 134 MB written per step > 126 MB), "
                   "no flush between steps (part of B stays L2-resident from the step before)",
-            "parallelism": (f"row shards x{world}, B replicated, no collective" if world > 1
-                            else "single GPU")}
+            "parallelism": par}
 
 
 def measured_peak():
@@ -216,7 +221,7 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": bench_config(A.nr, A.nnz, args.gpus),
+        "config": bench_config(A.nr, A.nnz, args.gpus, args.scaling),
         "variant": "cpuSpmvReference (spmvspmm_benchmark.cu:11-39), host",
         "cpu_baseline": {"value": round(gflops, 3), "unit": UNIT, "cores": cores, "kind": kind,
                          "sample": sample},
@@ -246,12 +251,22 @@ def run_ours(args):
     L = D.lib()
     alg = D.Alg[args.alg]
 
-    # Rank r owns row block r of an (N*262144) x 262144 matrix whose row
-    # blocks are independent power-law graphs; B is replicated once at setup
-    # (broadcast from rank 0), and no data crosses ranks per SpMM.
-    A = D.gen_powerlaw(NR, seed=rank)
-    dA = D.DeviceCsr(A, dev)
-    B = D.gen_dense(A.nc * NV, seed=1) if rank == 0 else None
+    # Weak scaling: rank r owns row block r of an (N*262144) x 262144 matrix
+    # whose row blocks are independent power-law graphs.  Strong scaling: the
+    # one 262,144-row matrix is cut into N row shards balanced by nonzeros +
+    # rows (daspmm.shard).  Either way B is replicated once at setup
+    # (broadcast from rank 0) and no data crosses ranks per SpMM.
+    strong = args.scaling == "strong" and world > 1
+    if strong:
+        from daspmm.shard import RowShardedSpmm
+        Afull = D.gen_powerlaw(NR, seed=0)
+        sh = RowShardedSpmm(Afull, rank, world, dev)
+        A, dA = sh.local, sh.dev
+        B = D.gen_dense(Afull.nc * NV, seed=1) if rank == 0 else None
+    else:
+        A = D.gen_powerlaw(NR, seed=rank)
+        dA = D.DeviceCsr(A, dev)
+        B = D.gen_dense(A.nc * NV, seed=1) if rank == 0 else None
     if pg:
         Bt = torch.from_numpy(B).to(dev) if rank == 0 else torch.empty(A.nc * NV, device=dev)
         from daspmm.shard import broadcast_dense
@@ -373,9 +388,10 @@ def run_ours(args):
         line = {
             "metric": METRIC, "value": round(gflops, 3), "unit": UNIT, "n_gpus": world,
             "steps": K, "warmup": args.warmup, "ms_per_step": round(ms_step, 5),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic",
-            "config": bench_config(A.nr, A.nnz, world),
+            "higher_is_better": True, "scaling": "strong" if strong else "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": bench_config(Afull.nr if strong else A.nr,
+                                   Afull.nnz if strong else A.nnz, world, args.scaling),
             "variant": dict(cfg_used.as_dict(), alg_name=alg.name),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4),
@@ -485,11 +501,44 @@ def run_variants(D, A, dA, Bt, dev, peak, K=20):
     return out
 
 
+def mixed_error(D, A, nv, Bt, vf, bf, vq, bq, scales, C):
+    """Error of a device result C against the host FP64 oracle, checked after
+    the timing on the leading rows the oracle holds (all rows where the
+    product has <= 2^25 elements; oracle.sample_rows): `kernel` (FP64 of the
+    stored inputs, per element against sum|a||b|) and `storage` (FP64 of the
+    FP32 inputs: norm_max, cond_max, rel_floored; oracle.error_stats)."""
+    import numpy as np
+    import torch
+    from oracle import oracle as O
+    R = O.sample_rows(A.rowPtr, A.colIdx, nv)
+    rp, ci, va32, cols = O.row_slice(A.rowPtr, A.colIdx, A.values, 0, R)
+    colt = torch.from_numpy(cols.astype(np.int64)).to(Bt.device)
+    b32 = Bt.view(A.nc, nv)[colt].cpu().numpy().reshape(-1)
+    p1 = int(A.rowPtr[R])
+    va64 = (va32.astype(np.float64) if vf == D.Fmt.F32 else
+            O.dequantize(int(vf), vq[:p1].cpu().view(torch.int16).numpy().view(np.uint16)))
+    if bf == D.Fmt.F32:
+        b64 = b32.astype(np.float64)
+    elif bf == D.Fmt.E4M3:
+        q = bq.view(A.nc, nv)[colt].cpu().numpy().reshape(-1)
+        b64 = (O.dequantize(3, q).reshape(-1, nv) *
+               scales.cpu().numpy().astype(np.float64)).reshape(-1)
+    else:
+        q = bq.view(A.nc, nv)[colt].cpu().view(torch.int16).numpy().view(np.uint16)
+        b64 = O.dequantize(int(bf), q.reshape(-1))
+    e = O.mixed_errors(rp, ci, va32, va64, b32, b64, C[: R * nv].cpu().numpy(), nv)
+    st = e["storage"]
+    return {"rows_checked": R, "kernel_cond_max": float("%.3g" % e["kernel"]),
+            "norm_max": float("%.3g" % st["norm_max"]),
+            "cond_max": float("%.3g" % st["cond_max"]),
+            "rel_floored": float("%.3g" % st["rel_floored"])}
+
+
 def run_mixed(D, A, dA, B, dev, steps, peak):
-    """Same SpMM with BF16 storage (values and B) and with BF16 values + FP8
-    E4M3 B (per-column scales): FP32 accumulation, kernel-timed.  Errors of
-    these forms against the FP64 oracle are stated by tests/test_mixed_gpu.py
-    (BF16 <= 1e-2, E4M3 <= 2^-4 max-norm relative)."""
+    """The same SpMM in FP32, with BF16 storage (values and B) and with BF16
+    values + FP8 E4M3 B (per-column scales); FP32 accumulation, kernel-timed.
+    Each result carries its error against the host FP64 oracle (mixed_error,
+    taken after the timing)."""
     import torch
     L = D.lib()
     Bt = torch.from_numpy(B).to(dev)
@@ -497,11 +546,15 @@ def run_mixed(D, A, dA, B, dev, steps, peak):
     out = {}
     C = torch.zeros(A.nr * NV, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
-    for name, vf, bf in (("bf16", D.Fmt.BF16, D.Fmt.BF16), ("bf16_e4m3", D.Fmt.BF16, D.Fmt.E4M3)):
-        vq = D.quantize(vt, vf)
+    for name, vf, bf in (("f32", D.Fmt.F32, D.Fmt.F32), ("bf16", D.Fmt.BF16, D.Fmt.BF16),
+                         ("bf16_e4m3", D.Fmt.BF16, D.Fmt.E4M3)):
+        vq = vt if vf == D.Fmt.F32 else D.quantize(vt, vf)
         scales = D.e4m3_scales(Bt, A.nc, NV) if bf == D.Fmt.E4M3 else None
-        bq = D.quantize(Bt, bf, scales, NV if scales is not None else 0)
-        run = lambda: D.spmm_mixed(dA, vq, vf, bq, bf, C, NV, b_scales=scales, stream=stream)
+        bq = Bt if bf == D.Fmt.F32 else D.quantize(Bt, bf, scales, NV if scales is not None else 0)
+        if vf == D.Fmt.F32:
+            run = lambda: D.spmm(D.Alg.CSR_BALANCED, 0, dA, Bt, C, nv=NV, stream=stream)
+        else:
+            run = lambda: D.spmm_mixed(dA, vq, vf, bq, bf, C, NV, b_scales=scales, stream=stream)
         for _ in range(5):
             run()
         torch.cuda.synchronize(dev)
@@ -516,12 +569,16 @@ def run_mixed(D, A, dA, B, dev, steps, peak):
         n = L.daspmm_kernel_timer_end(kt, steps)
         ms = s.elapsed_time(e) / steps
         kms = sum(kt) / max(1, n)
-        sb = 2 if bf == D.Fmt.BF16 else 1
-        abytes = algorithmic_bytes(A, NV, s_val=2, s_b=sb) + (4 * NV if sb == 1 else 0)
+        sv = 4 if vf == D.Fmt.F32 else 2
+        sb = {D.Fmt.F32: 4, D.Fmt.BF16: 2, D.Fmt.E4M3: 1}[bf]
+        abytes = algorithmic_bytes(A, NV, s_val=sv, s_b=sb) + (4 * NV if sb == 1 else 0)
         out[name] = {"value": round(2.0 * A.nnz * NV / (ms * 1e-3) / 1e9, 3), "unit": UNIT,
                      "ms_per_step": round(ms, 5), "kernel_ms": round(kms, 5),
                      "algorithmic_bytes": abytes,
-                     "roofline_frac": round(abytes / (kms * 1e-3) / 1e9 / peak, 4)}
+                     "roofline_frac": round(abytes / (kms * 1e-3) / 1e9 / peak, 4),
+                     "err_vs_fp64": mixed_error(D, A, NV, Bt, vf, bf, vq, bq, scales, C)}
+    out["speedup_vs_f32"] = {k: round(out["f32"]["ms_per_step"] / out[k]["ms_per_step"], 3)
+                             for k in ("bf16", "bf16_e4m3")}
     return out
 
 
@@ -529,12 +586,13 @@ def run_mixed_random(D, dev, peak, steps: int = 10):
     """The second mixed-precision matrix: 1,048,576 rows, uniform random
     columns, average degree 8 (Poisson row lengths, seed 0); N in {32, 128,
     512}; FP32, BF16 values and B, BF16 values + E4M3 B.  Device time of the
-    SpMM per call (library timer), GFLOP/s and the fraction of the measured
-    HBM copy bandwidth its algorithmic bytes reach."""
+    SpMM per call (library timer), GFLOP/s, the fraction of the measured
+    HBM copy bandwidth its algorithmic bytes reach, and the error against the
+    host FP64 oracle (mixed_error) of every result."""
     import torch
     L = D.lib()
     A = D.gen_random(1 << 20, 1 << 20, 8.0, seed=0)
-    dA = D.DeviceCsr(A, dev)
+    dA = D.DeviceCsr(A)
     g = torch.Generator(device=dev)
     g.manual_seed(0)
     vq = D.quantize(dA.values, D.Fmt.BF16)
@@ -546,13 +604,16 @@ def run_mixed_random(D, dev, peak, steps: int = 10):
         sc = D.e4m3_scales(Bt, A.nc, nv)
         b8 = D.quantize(Bt, D.Fmt.E4M3, sc, nv)
         runs = {
-            "f32": (lambda: D.spmm(D.Alg.CSR_BALANCED, 0, dA, Bt, C, nv=nv), 4, 4),
-            "bf16": (lambda: D.spmm_mixed(dA, vq, D.Fmt.BF16, b16, D.Fmt.BF16, C, nv), 2, 2),
+            "f32": (lambda: D.spmm(D.Alg.CSR_BALANCED, 0, dA, Bt, C, nv=nv), 4, 4,
+                    (D.Fmt.F32, D.Fmt.F32, dA.values, Bt, None)),
+            "bf16": (lambda: D.spmm_mixed(dA, vq, D.Fmt.BF16, b16, D.Fmt.BF16, C, nv), 2, 2,
+                     (D.Fmt.BF16, D.Fmt.BF16, vq, b16, None)),
             "bf16_e4m3": (lambda: D.spmm_mixed(dA, vq, D.Fmt.BF16, b8, D.Fmt.E4M3, C, nv,
-                                               b_scales=sc), 2, 1),
+                                               b_scales=sc), 2, 1,
+                          (D.Fmt.BF16, D.Fmt.E4M3, vq, b8, sc)),
         }
         res = {}
-        for name, (run, s_val, s_b) in runs.items():
+        for name, (run, s_val, s_b, (vf, bf, vv, bb, ss)) in runs.items():
             for _ in range(3):
                 run()
             torch.cuda.synchronize(dev)
@@ -568,7 +629,8 @@ def run_mixed_random(D, dev, peak, steps: int = 10):
             res[name] = {"gflops": round(2.0 * A.nnz * nv / (kms * 1e-3) / 1e9, 1),
                          "ms": round(kms, 4),
                          "roofline_frac": round(abytes / (kms * 1e-3) / 1e9 / peak, 4),
-                         "gather_bound_frac": round(gbytes / (kms * 1e-3) / 1e9 / peak, 4)}
+                         "gather_bound_frac": round(gbytes / (kms * 1e-3) / 1e9 / peak, 4),
+                         "err_vs_fp64": mixed_error(D, A, nv, Bt, vf, bf, vv, bb, ss, C)}
         out[f"n{nv}"] = res
         del Bt, C, b16, b8
     return out
@@ -652,18 +714,21 @@ def run_batched(D, dev, reps: int = 20):
 def run_serving(D, dev, seconds: float = 1.0, rate: float = 20000.0):
     """The serving configuration: a pool of 64 resident matrices (rows
     log-uniform in [1k, 262k], half uniform-random, half power-law), requests
-    with N drawn from {16, 64, 256}, Poisson arrivals at `rate` per second
-    (seed 0).  Served with continuous batching (FP32 values, BF16 B, FP32
-    accumulate) and, as the baseline, one plain FP32 launch per request; both
-    through the same native server (queue, HBM-budget admission, dispatcher
-    thread).  Also the capacity of each: every request queued at t = 0."""
+    with N drawn from {16, 64, 256}, Poisson arrivals (seed 0).  Served with
+    continuous batching (FP32 values, BF16 B, FP32 accumulate) and, as the
+    baseline, one plain FP32 launch per request; both through the same native
+    server (queue, HBM-budget admission, dispatcher thread).  Reported: both
+    modes at `rate`; each mode's capacity (every request queued at t = 0); an
+    offered-rate sweep; throughput at equal p99 (the bound is the plain path's
+    p99 at half its capacity; the batched mode's highest offered rate that
+    keeps up within that p99, found by bisection); and the batched mode at a
+    high rate for 1..4 launch groups in flight."""
     import numpy as np
     import torch
     import daspmm.workloads as WL
     pool = WL.config5_pool(64)
-    rng = np.random.default_rng(0)
     nvs = (16, 64, 256)
-    dmats = [D.DeviceCsr(A, dev) for A in pool]
+    dmats = [D.DeviceCsr(A) for A in pool]
     touched = [A.cols_touched() for A in pool]
     g = torch.Generator(device=dev)
     g.manual_seed(0)
@@ -673,48 +738,84 @@ def run_serving(D, dev, seconds: float = 1.0, rate: float = 20000.0):
             b = torch.empty(A.nc * nv, device=dev).uniform_(-1, 1, generator=g)
             B32[i, nv] = b
             B16[i, nv] = D.quantize(b, D.Fmt.BF16)
-    n = int(rate * seconds)
-    arrivals = WL.poisson_arrivals(rate, n, seed=0)
-    pick = rng.integers(0, len(pool), n)
-    pnv = rng.choice(nvs, n)
-    flop = sum(2.0 * pool[m].nnz * int(v) for m, v in zip(pick, pnv))
+
+    def stream_of(r, n=None):
+        """n requests at Poisson rate r (seed 0): arrivals, matrix ids, N."""
+        n = n or max(200, int(r * seconds))
+        rng = np.random.default_rng(0)
+        return (WL.poisson_arrivals(r, n, seed=0), rng.integers(0, len(pool), n),
+                rng.choice(nvs, n))
 
     def bytes_of(m, nv, s_b):
         A = pool[m]
         return A.nnz * 8 + 4 * (A.nr + 1) + touched[m] * nv * s_b + A.nr * nv * 4
 
-    def run(mode, b_fmt, Bs, s_b, arr):
-        srv = D.Server(budget_bytes=8 << 30, mode=mode, b_fmt=b_fmt)
+    def run(mode, r, zero=False, max_inflight=0):
+        batched = mode == D.ServeMode.BATCHED
+        b_fmt, Bs, s_b = (D.Fmt.BF16, B16, 2) if batched else (D.Fmt.F32, B32, 4)
+        arr, pick, pnv = stream_of(r)
+        if zero:
+            arr = np.zeros(arr.size)
+        srv = D.Server(budget_bytes=8 << 30, mode=mode, b_fmt=b_fmt, max_inflight=max_inflight)
         ids = [srv.add_matrix(dA) for dA in dmats]
         reqs = [(ids[m], int(v), Bs[int(m), int(v)]) for m, v in zip(pick, pnv)]
         srv.replay(reqs[:200], np.zeros(200), release=True)       # warm-up
         res = srv.replay(reqs, arr, release=True)
         st = srv.stats()
         srv.close()
-        lat = np.array([r.latency_us for r in res])
-        ok = sum(r.status == 0 for r in res)
+        lat = np.array([q.latency_us for q in res])
+        ok = sum(q.status == 0 for q in res)
         span = float(np.max(arr + lat * 1e-6))
+        flop = sum(2.0 * pool[m].nnz * int(v) for m, v in zip(pick, pnv))
         nbytes = sum(bytes_of(int(m), int(v), s_b) for m, v in zip(pick, pnv))
-        return {"req_s": round(ok / span, 1), "gflops": round(flop / span / 1e9, 1),
-                "gbs": round(nbytes / span / 1e9, 1),
+        return {"offered_req_s": None if zero else round(r, 1), "req_s": round(ok / span, 1),
+                "gflops": round(flop / span / 1e9, 1), "gbs": round(nbytes / span / 1e9, 1),
                 "p50_us": round(float(np.percentile(lat, 50)), 1),
                 "p99_us": round(float(np.percentile(lat, 99)), 1),
                 "completed": int(ok), "groups": int(st["groups"]),
                 "mean_group": round(st["launched"] / max(1, st["groups"]), 2),
                 "max_group": int(st["max_group"])}
 
+    B_, P_ = D.ServeMode.BATCHED, D.ServeMode.PLAIN
+    n = int(rate * seconds)
     out = {"pool": len(pool), "requests": n, "offered_req_s": rate, "nv": list(nvs),
            "pool_nnz": int(sum(A.nnz for A in pool)),
-           "batched_bf16": run(D.ServeMode.BATCHED, D.Fmt.BF16, B16, 2, arrivals),
-           "plain_fp32": run(D.ServeMode.PLAIN, D.Fmt.F32, B32, 4, arrivals)}
-    zero = np.zeros(n)
-    cap_b = run(D.ServeMode.BATCHED, D.Fmt.BF16, B16, 2, zero)
-    cap_p = run(D.ServeMode.PLAIN, D.Fmt.F32, B32, 4, zero)
+           "batched_bf16": run(B_, rate), "plain_fp32": run(P_, rate)}
+    cap_b = run(B_, rate, zero=True)
+    cap_p = run(P_, rate, zero=True)
     out["capacity"] = {"batched_bf16_req_s": cap_b["req_s"], "plain_fp32_req_s": cap_p["req_s"],
                        "batched_bf16_gflops": cap_b["gflops"],
                        "plain_fp32_gflops": cap_p["gflops"],
                        "batched_mean_group": cap_b["mean_group"],
                        "ratio": round(cap_b["req_s"] / max(cap_p["req_s"], 1e-9), 3)}
+    # throughput at equal p99: the plain path at half its capacity sets the bound
+    half = 0.5 * cap_p["req_s"]
+    plain_half = run(P_, half)
+    bound = plain_half["p99_us"]
+    keeps_up = lambda q, r: q["p99_us"] <= bound and q["req_s"] >= 0.97 * r
+    lo, hi = half, 4.0 * cap_b["req_s"]
+    best = run(B_, lo)
+    if keeps_up(best, lo):
+        for _ in range(6):
+            mid = 0.5 * (lo + hi)
+            q = run(B_, mid)
+            if keeps_up(q, mid):
+                lo, best = mid, q
+            else:
+                hi = mid
+    out["equal_p99"] = {"p99_bound_us": bound, "plain_req_s": plain_half["req_s"],
+                        "plain_p99_us": plain_half["p99_us"],
+                        "batched_req_s": best["req_s"], "batched_p99_us": best["p99_us"],
+                        "batched_offered_req_s": best["offered_req_s"],
+                        "ratio": round(best["req_s"] / max(plain_half["req_s"], 1e-9), 3),
+                        "rule": "bound = plain FP32 p99 at half its capacity; batched: the "
+                                "highest offered Poisson rate (bisection) whose p99 stays "
+                                "within the bound and whose throughput keeps up (>= 97%)"}
+    out["sweep"] = {"batched_bf16": [run(B_, r) for r in (10e3, 20e3, 40e3, 60e3, 80e3)],
+                    "plain_fp32": [run(P_, r) for r in (5e3, 10e3, 15e3, 20e3)]}
+    hot = 0.9 * cap_b["req_s"]
+    out["max_inflight"] = {"offered_req_s": round(hot, 1),
+                           **{str(k): run(B_, hot, max_inflight=k) for k in (1, 2, 3, 4)}}
     return out
 
 
@@ -790,6 +891,9 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--scaling", choices=["weak", "strong"], default="weak",
+                    help="N > 1: one 262144-row block per rank (weak) or the one matrix cut "
+                         "into N row shards (strong)")
     ap.add_argument("--no-refk", action="store_true",
                     help="skip the reference's own kernels and cuSPARSE comparison lines")
     ap.add_argument("--no-variants", action="store_true",

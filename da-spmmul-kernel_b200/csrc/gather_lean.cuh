@@ -455,23 +455,76 @@ __global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_fast(const KArgs 
 
 // ---------------------------------------------------------------- half-warp form
 // VL floats: plain / L2-hinted stores and L2-coherent loads, VL <= 8.
+// (VL = 16: two 32-byte accesses)
 template <int VL>
 __device__ __forceinline__ void st_n(float *p, const float (&r)[VL])
 {
-    if constexpr (VL == 8) st8(p, r);
-    else st_v<VL>(p, r);
+    if constexpr (VL == 16) {
+        st8(p, *reinterpret_cast<const float(*)[8]>(&r[0]));
+        st8(p + 8, *reinterpret_cast<const float(*)[8]>(&r[8]));
+    } else if constexpr (VL == 8) {
+        st8(p, r);
+    } else {
+        st_v<VL>(p, r);
+    }
 }
 template <int VL>
 __device__ __forceinline__ void st_hint_n(float *p, const float (&r)[VL], uint64_t pol)
 {
-    if constexpr (VL == 8) st8_hint(p, r, pol);
-    else st_hint<VL>(p, r, pol);
+    if constexpr (VL == 16) {
+        st8_hint(p, *reinterpret_cast<const float(*)[8]>(&r[0]), pol);
+        st8_hint(p + 8, *reinterpret_cast<const float(*)[8]>(&r[8]), pol);
+    } else if constexpr (VL == 8) {
+        st8_hint(p, r, pol);
+    } else {
+        st_hint<VL>(p, r, pol);
+    }
 }
 template <int VL>
 __device__ __forceinline__ void ld_cg_n(float (&r)[VL], const float *p)
 {
-    if constexpr (VL == 8) ld8_cg(r, p);
-    else ld_cg<VL>(r, p);
+    if constexpr (VL == 16) {
+        ld8_cg(*reinterpret_cast<float(*)[8]>(&r[0]), p);
+        ld8_cg(*reinterpret_cast<float(*)[8]>(&r[8]), p + 8);
+    } else if constexpr (VL == 8) {
+        ld8_cg(r, p);
+    } else {
+        ld_cg<VL>(r, p);
+    }
+}
+
+// NW 32-bit words (NW = 8: one 32-byte load, 4: one 16-byte load) of B,
+// read-only path, left packed; elem<TB>() unpacks element i as a float.
+template <int NW>
+__device__ __forceinline__ void ld_raw(uint32_t (&w)[NW], const void *p)
+{
+    if constexpr (NW == 8) {
+        float f[8];
+        ld8_nc(f, reinterpret_cast<const float *>(p));
+#pragma unroll
+        for (int i = 0; i < 8; ++i) w[i] = __float_as_uint(f[i]);
+    } else {
+        static_assert(NW == 4, "16- or 32-byte lane loads");
+        const uint4 t = __ldg(reinterpret_cast<const uint4 *>(p));
+        w[0] = t.x; w[1] = t.y; w[2] = t.z; w[3] = t.w;
+    }
+}
+template <typename TB, int NW>
+__device__ __forceinline__ float elem(const uint32_t (&w)[NW], int i)
+{
+    if constexpr (std::is_same<TB, float>::value) {
+        return __uint_as_float(w[i]);
+    } else if constexpr (std::is_same<TB, bf16>::value) {
+        const uint32_t x = w[i >> 1];
+        return __uint_as_float((i & 1) ? (x & 0xFFFF0000u) : (x << 16));
+    } else if constexpr (std::is_same<TB, fp16>::value) {
+        return __half2float(__ushort_as_half((unsigned short)(w[i >> 1] >> (16 * (i & 1)))));
+    } else {  // fp8 e4m3 (element pairs share one conversion; see elem2)
+        const __half2_raw h2 = __nv_cvt_fp8x2_to_halfraw2(
+            (__nv_fp8x2_storage_t)(w[i >> 2] >> (8 * (i & 2))), __NV_E4M3);
+        const float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&h2));
+        return (i & 1) ? f.y : f.x;
+    }
 }
 
 // piece_arrive for a G-lane worker of a warp (lanes of `gmask`, VL floats per
@@ -517,37 +570,43 @@ static __device__ __noinline__ void piece_arrive_grp(const int *__restrict__ row
 #ifndef DASPMM_GRP_U
 #define DASPMM_GRP_U 8      // nonzeros in flight per worker step
 #endif
+#ifndef DASPMM_GRP_U16
+#define DASPMM_GRP_U16 8    // the same for 2- and 1-byte B (16 elements per lane load)
+#endif
 #ifndef DASPMM_GRP_MINB
 #define DASPMM_GRP_MINB 2   // CTAs of 256 threads per SM: 16 warps, <= 128 registers
 #endif
 
-// k_bal_fast with G-lane workers: FP32, column tiles of 8*G floats (G = 16:
-// 128, 8: 64, 4: 32), beta == 0, B and C 32-byte aligned.  Each worker (G
-// consecutive lanes) takes one chunk of a group (32/G consecutive chunks per
-// warp) and covers its tile of a B row with G lanes x 32-byte loads
-// (ld.global.nc.v8.f32), so one warp instruction gathers 32/G nonzeros -- 256
-// bytes per lane-load whatever the tile width.  The workers run in step: the
-// window loop runs to the longest chunk of the group (balanced chunks differ
-// by a few nonzeros); a worker past its chunk's end gathers padding (column
-// 0, value 0) and stores nothing.  Windows are G nonzeros (lane l of a
-// worker ends row r + l), gathered min(U, G) B rows at a time.  Everything
-// else is k_bal_fast's: same chunks, carries, split-row
-// combine and order of summation, so results are bit-identical to it.
-// Column tiles are blockIdx.y: the CTAs of tile 0 are dispatched first, so
-// with several tiles their B column slabs are gathered one after the other
-// (each slab a fraction of B in L2).
-template <int G, int U, typename TV = float, typename TB = float>
+// k_bal_fast with G-lane workers, beta == 0.  Each worker (G consecutive
+// lanes) takes one chunk of a group (32/G consecutive chunks per warp) and
+// covers its column tile of a B row with G lanes x one 16- or 32-byte load
+// of EPL elements each (FP32: 8 per 32 bytes; BF16 / FP16: 16 per 32 bytes;
+// E4M3: 16 per 16 bytes), so the tile is G*EPL columns and one warp
+// instruction gathers 32/G nonzeros.  FP32 uses G = 16 for 128-column tiles
+// and G = 8 for 64; BF16 / FP16 / E4M3 reach 128 columns with G = 8.  The
+// workers run in step: the window loop runs to the longest chunk of the group
+// (balanced chunks differ by a few nonzeros); a worker past its chunk's end
+// gathers padding (column 0, value 0) and stores nothing.  Windows are G
+// nonzeros (lane l of a worker ends row r + l), gathered min(U, G) B rows at a
+// time, each row's EPL elements unpacked to FP32 as they are summed.
+// Everything else is k_bal_fast's: same chunks, carries, split-row combine
+// and order of summation (FP32 products and sums), so results are
+// bit-identical to it.  Column tiles are blockIdx.y: the CTAs of tile 0 are
+// dispatched first, so with several tiles their B column slabs are gathered
+// one after the other.  B aligned to EPL*sizeof(TB) bytes, C and the carry
+// slots to 32 bytes.
+template <int G, int EPL, int U, typename TV = float, typename TB = float>
 __global__ void __launch_bounds__(256, DASPMM_GRP_MINB) k_bal_grp(const KArgs a)
 {
-    constexpr int VL = 8;              // floats per lane: one 32-byte load
-    constexpr int NW = 32 / G;         // workers per warp
-    constexpr int UU = U < G ? U : G;  // rows in flight per step (within one window)
+    constexpr int NW = 32 / G;                             // workers per warp
+    constexpr int RAW = EPL * (int)sizeof(TB) / 4;         // 32-bit words per lane load
+    constexpr int UU = U < G ? U : G;                      // rows in flight per step
     constexpr unsigned GM = G == 32 ? 0xFFFFFFFFu : ((1u << G) - 1u);
     constexpr bool SCALED = std::is_same<TB, fp8>::value;
     const int lane = threadIdx.x & 31, w = lane / G, gl = lane % G;
     const unsigned gmask = GM << (G * w);
     const int tile = blockIdx.y, tiles = gridDim.y;
-    const int tb = tile * (G * VL) + gl * VL;
+    const int tb = tile * (G * EPL) + gl * EPL;
     const TB *Bl = reinterpret_cast<const TB *>(a.B) + tb;
     const TV *Av = reinterpret_cast<const TV *>(a.vals);
     const uint64_t pol_once = policy_evict_first();
@@ -556,9 +615,9 @@ __global__ void __launch_bounds__(256, DASPMM_GRP_MINB) k_bal_grp(const KArgs a)
 
     pdl_trigger();  // the list-mode walk may be scheduled; it waits for this grid
     pdl_wait();     // the boundaries from k_partition are complete
-    float sc[VL];   // read after the wait, like every input
+    float sc[SCALED ? EPL : 1];  // read after the wait, like every input
 #pragma unroll
-    for (int e = 0; e < VL; ++e) sc[e] = SCALED ? __ldg(a.bscale + tb + e) : 1.0f;
+    for (int e = 0; e < (SCALED ? EPL : 1); ++e) sc[e] = SCALED ? __ldg(a.bscale + tb + e) : 1.0f;
     // padding (column 0, value 0) adds nothing unless row 0 of B holds an Inf
     // or NaN; then every chunk is handed to the walk kernel (as in k_bal_fast).
     // Without nonzeros nothing is padded (and B may have no rows).
@@ -612,9 +671,9 @@ __global__ void __launch_bounds__(256, DASPMM_GRP_MINB) k_bal_grp(const KArgs a)
         for (int o = G; o < 32; o <<= 1) nwin = max(nwin, __shfl_xor_sync(kFull, nwin, o));
         bool cont = !skip && k0 > rstart;
         const bool head_piece = cont;
-        float acc[VL];
+        float acc[EPL];
 #pragma unroll
-        for (int e = 0; e < VL; ++e) acc[e] = 0.0f;
+        for (int e = 0; e < EPL; ++e) acc[e] = 0.0f;
         auto load_win = [&](int wb, int &col, float &val) {
             const bool ok = wb + gl < ke;
             col = ok ? ld_hint_s32(a.colIdx + wb + gl, pol_once) : 0;
@@ -643,21 +702,22 @@ __global__ void __launch_bounds__(256, DASPMM_GRP_MINB) k_bal_grp(const KArgs a)
                     cc[u] = __shfl_sync(kFull, ccur, g * UU + u, G);
                     vv[u] = __shfl_sync(kFull, vcur, g * UU + u, G);
                 }
-                float b[UU][VL];
+                uint32_t b[UU][RAW];
 #pragma unroll
-                for (int u = 0; u < UU; ++u) ld_b<TB, VL>(b[u], Bl + (size_t)cc[u] * a.ldb);
+                for (int u = 0; u < UU; ++u) ld_raw<RAW>(b[u], Bl + (size_t)cc[u] * a.ldb);
 #pragma unroll
                 for (int u = 0; u < UU; ++u) {
 #pragma unroll
-                    for (int e = 0; e < VL; ++e) acc[e] = fmaf(vv[u], b[u][e], acc[e]);
+                    for (int e = 0; e < EPL; ++e)
+                        acc[e] = fmaf(vv[u], elem<TB, RAW>(b[u], e), acc[e]);
                     if ((ends >> (g * UU + u)) & 1u) {
                         if constexpr (SCALED) {
 #pragma unroll
-                            for (int e = 0; e < VL; ++e) acc[e] *= sc[e];
+                            for (int e = 0; e < EPL; ++e) acc[e] *= sc[e];
                         }
-                        st_hint_n<VL>(cdst, acc, pol_once);
+                        st_hint_n<EPL>(cdst, acc, pol_once);
 #pragma unroll
-                        for (int e = 0; e < VL; ++e) acc[e] = 0.0f;
+                        for (int e = 0; e < EPL; ++e) acc[e] = 0.0f;
                         cont = false;
                         ++r;
                         cdst = a.C + (size_t)r * a.ldc + tb;
@@ -674,16 +734,16 @@ __global__ void __launch_bounds__(256, DASPMM_GRP_MINB) k_bal_grp(const KArgs a)
             tail_piece = !cont;  // a continuing row here is the head piece itself
             if constexpr (SCALED) {
 #pragma unroll
-                for (int e = 0; e < VL; ++e) acc[e] *= sc[e];
+                for (int e = 0; e < EPL; ++e) acc[e] *= sc[e];
             }
-            st_n<VL>(slot_ptr(a, c, cont ? 0 : 1, tb), acc);
+            st_n<EPL>(slot_ptr(a, c, cont ? 0 : 1, tb), acc);
         }
         if (head_piece)
-            piece_arrive_grp<G, VL, TV, TB>(a.rowPtr, a.cnt, a.slots, a.C, a.ldc, a.nv, a.chunk,
-                                            r0, tb, tiles, tile, gmask);
+            piece_arrive_grp<G, EPL, TV, TB>(a.rowPtr, a.cnt, a.slots, a.C, a.ldc, a.nv, a.chunk,
+                                             r0, tb, tiles, tile, gmask);
         if (tail_piece)
-            piece_arrive_grp<G, VL, TV, TB>(a.rowPtr, a.cnt, a.slots, a.C, a.ldc, a.nv, a.chunk,
-                                            s1, tb, tiles, tile, gmask);
+            piece_arrive_grp<G, EPL, TV, TB>(a.rowPtr, a.cnt, a.slots, a.C, a.ldc, a.nv, a.chunk,
+                                             s1, tb, tiles, tile, gmask);
         __syncwarp();
         unsigned int nx = 0;
         if (lane == 0) nx = atomicAdd(a.head + tile, 1u);
@@ -722,29 +782,35 @@ inline void launch_lean(const Resolved &r, KArgs a, cudaStream_t st)
         1, std::min<long long>(((long long)a.nchunks + 7) / 8, resident));
     if (!K && a.beta == 0.0f) {
         a.list_mode = 0;
-        // the worker-group kernel: G = W / 8 lanes per chunk, 32-byte loads of
-        // B, 32-byte stores of C and carries
-        constexpr int G = W / 8;
+        // the worker-group kernel: EPL elements of B per lane load (FP32: 8 in
+        // 32 bytes; BF16 / FP16: 16 in 32 bytes; E4M3: 16 in 16 bytes),
+        // G = W / EPL lanes per chunk; stores of C and carries 32-byte aligned
+        constexpr bool f32 = std::is_same<TV, float>::value && std::is_same<TB, float>::value;
+        constexpr int EPL = std::is_same<TB, float>::value ? 8 : 16;
+        constexpr int G = W / EPL;
         const bool aligned_g =
-            (reinterpret_cast<uintptr_t>(a.B) % 32) == 0 &&
+            (reinterpret_cast<uintptr_t>(a.B) % (EPL * sizeof(TB))) == 0 &&
             ((reinterpret_cast<uintptr_t>(a.C) | reinterpret_cast<uintptr_t>(a.slots)) % 32) ==
                 0 &&
-            a.ldb % 8 == 0 && a.ldc % 8 == 0 && a.nv % W == 0;
-        constexpr bool f32 = std::is_same<TV, float>::value && std::is_same<TB, float>::value;
+            a.ldb % EPL == 0 && a.ldc % 8 == 0 && a.nv % W == 0;
         // measured on the 262k power-law matrix: the group form wins for FP32
         // storage and 128- or 64-column tiles (N = 128: 84 against 113 us,
-        // N = 64: 54 against 61 us); for 32-column tiles (G = 4) the 32-lane
-        // kernel is as fast or faster (41 against 42 us at N = 32).  BF16 /
-        // E4M3 B (16- / 8-byte lane loads in the half-warp form) ran slower
-        // than k_bal_fast.
-        if (f32 && W >= 64 && DASPMM_GRP && aligned_g) {
-            constexpr int NW = 32 / G;
-            const long long groups = ((long long)a.nchunks + NW - 1) / NW;
+        // N = 64: 54 against 61 us); for 32-column FP32 tiles (G = 4) the
+        // 32-lane kernel is as fast or faster (41 against 42 us at N = 32).
+        // BF16 / FP16 / E4M3 B: the group form wins from two 128-column tiles
+        // on (BF16 N = 256: 155 against 173 us, N = 512: 282 against 335;
+        // E4M3 N = 512: 239 against 318), the 32-lane kernel for one (BF16
+        // N = 128: 77 against 84 us; E4M3 equal).
+        constexpr bool grp_ok = f32 ? W >= 64 : W == 128;
+        if (grp_ok && DASPMM_GRP && aligned_g && (f32 || r.tiles >= 2)) {
+            constexpr int NWK = 32 / (grp_ok ? G : 32);
+            const long long groups = ((long long)a.nchunks + NWK - 1) / NWK;
             const unsigned gg = (unsigned)std::max<long long>(
                 1, std::min<long long>((groups + 7) / 8,
                                        (long long)device_sms() * DASPMM_GRP_MINB));
-            if constexpr (f32 && W >= 64)
-                launch_pdl(k_bal_grp<G, DASPMM_GRP_U>, dim3(gg, r.tiles), st, a);
+            if constexpr (grp_ok)
+                launch_pdl(k_bal_grp<G, EPL, f32 ? DASPMM_GRP_U : DASPMM_GRP_U16, TV, TB>,
+                           dim3(gg, r.tiles), st, a);
         } else if constexpr (W == 128) {
             launch_pdl(k_bal_fast<W, DASPMM_LEAN_U, TV, TB>, dim3(gx, r.tiles), st, a);
         } else {  // one queue of (tile, chunk) items

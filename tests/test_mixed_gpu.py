@@ -216,3 +216,28 @@ def test_config3_full_size_error_bound(cuda):
                     assert e["storage"]["cond_max"] <= O.MIXED_TOL, what
                 del vq, bq
             del Bt, C
+
+
+def test_group_kernel_equals_32_lane_kernel_mixed(mats):
+    """Reduced-precision B with two or more 128-column tiles runs the worker-
+    group window kernel when C is 32-byte aligned, the 32-lane one when C is
+    16 bytes off: same chunks and order of summation, bit-identical C."""
+    import torch
+    rng = np.random.default_rng(31)
+    for name in ("powerlaw", "random"):
+        A, dA = mats[name]
+        for nv in (128, 256, 384):
+            B = rng.uniform(-1, 1, A.nc * nv).astype(np.float32)
+            for vf, bf in ((D.Fmt.BF16, D.Fmt.BF16), (D.Fmt.F16, D.Fmt.F16),
+                           (D.Fmt.BF16, D.Fmt.E4M3), (D.Fmt.F32, D.Fmt.E4M3)):
+                vq, bq, scales, v64, b64 = _quant_inputs(A, B, vf, bf, nv)
+                Ca = torch.full((A.nr * nv,), float("nan"), device="cuda")
+                Cbuf = torch.full((A.nr * nv + 8,), float("nan"), device="cuda")
+                Co = Cbuf[4:4 + A.nr * nv]
+                assert Ca.data_ptr() % 32 == 0 and Co.data_ptr() % 32 == 16
+                for C in (Ca, Co):
+                    D.spmm_mixed(dA, vq, vf, bq, bf, C, nv, b_scales=scales)
+                torch.cuda.synchronize()
+                assert torch.equal(Ca, Co), f"{name} nv={nv} {vf.name}/{bf.name}"
+                eq, e64 = _errors(A, nv, B, Ca.cpu().numpy(), v64, b64)
+                assert eq <= O.REL_TOL_F32 and e64 <= _tol(bf)
