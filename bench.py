@@ -277,10 +277,16 @@ def run_ours(args):
     stream = torch.cuda.current_stream(dev)
     cfg = D.default_config(alg, 0, A.nr, A.nc, A.nnz, NV) if alg != D.Alg.AUTO else None
 
-    def step():
-        D.spmm(alg, 0, dA, Bt, Ct, beta=0.0, nv=NV, stream=stream, cfg=None)
+    # the library's default point unless a tile width / chunk size is asked for
+    step_cfg = None
+    if alg != D.Alg.AUTO and (args.lanes_col or args.chunk):
+        step_cfg = D.Config(alg=int(alg), lanes_col=args.lanes_col, chunk=args.chunk)
 
-    # warm-up steps, then a ~1.5 s burst so clocks settle (both untimed)
+    def step():
+        D.spmm(alg, 0, dA, Bt, Ct, beta=0.0, nv=NV, stream=stream, cfg=step_cfg)
+
+    # warm-up steps (untimed), then the timed region: K back-to-back SpMMs,
+    # CUDA events around all of them on the launching stream
     for _ in range(max(3, args.warmup)):
         step()
     torch.cuda.synchronize(dev)
@@ -293,13 +299,8 @@ def run_ours(args):
         gpu_uuid = None
     sampler = ClockSampler(gpu_uuid)
     sampler.start()
-    t_burst = time.time()
-    while time.time() - t_burst < 1.5:
-        for _ in range(200):
-            step()
-        torch.cuda.synchronize(dev)
+    time.sleep(0.25)  # the sampler's first sample lands before the timed region
 
-    # the timed region: K back-to-back SpMMs, CUDA events around all of them
     K = args.steps
     if pg:
         pg.barrier()
@@ -317,12 +318,29 @@ def run_ours(args):
     if pg:
         pg.barrier()
     launches = L.daspmm_launch_count() - launches0
+
+    # The timed region (K x ~0.09 ms) is shorter than one clock sample, so
+    # the same step runs on for >= 1.2 s right after it, sampled by the clock
+    # record; its own event time is the sustained rate under the power cap.
+    e_s0, e_s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t_s0 = time.time()
+    e_s0.record(stream)
+    n_sus = 0
+    while time.time() - t_s0 < 1.2:
+        for _ in range(200):
+            step()
+        n_sus += 200
+        torch.cuda.synchronize(dev)
+    e_s1.record(stream)
+    torch.cuda.synchronize(dev)
+    t_s1 = time.time()
+    sus_ms = e_s0.elapsed_time(e_s1) / n_sus
     sampler.stop()
 
-    # the SpMM's own device time (k_partition to the list walk), from
-    # library-owned events recorded on the launching stream around each call,
-    # over a second pass of K calls: per-call events inside the timed region
-    # would stand between the SpMMs and stop their kernels from overlapping
+    # the main gather kernel's own device time, from library-owned events
+    # recorded on the launching stream around each launch of it, over a
+    # second pass of K calls: per-call events inside the timed region would
+    # stand between the SpMMs and stop their kernels from overlapping
     D.check(L.daspmm_kernel_timer_begin(K), "kernel_timer_begin")
     for _ in range(K):
         step()
@@ -369,9 +387,21 @@ def run_ours(args):
             cpu = {"value": round(2.0 * nnz_s * NV / (ms_cpu * 1e-3) / 1e9, 3), "unit": UNIT,
                    "cores": cores, "kind": kind,
                    "sample": f"full matrix ({nnz_s} nnz, N=128), median of 3 passes, 1 thread"}
-        refk, cus = (None, None) if (args.no_refk or world > 1) else \
-            run_reference_kernels(A, dA, Bt, dev, ms_step)
-        variants = None if (args.no_variants or world > 1) else run_variants(D, A, dA, Bt, dev, peak)
+        # NVTX ranges name the sections for a profiler's kernel filter
+        # (ncu --nvtx --nvtx-include "variants/")
+        nvtx = torch.cuda.nvtx
+        refk, cus = None, None
+        if not (args.no_refk or world > 1):
+            nvtx.range_push("reference_kernels")
+            refk, cus = run_reference_kernels(A, dA, Bt, dev, ms_step)
+            nvtx.range_pop()
+        plan = None if world > 1 else run_plan(D, A, dA, Bt, dev, peak, K)
+        l2win = None if (args.no_variants or world > 1) else run_l2_window(D, A, dA, Bt, dev, peak)
+        variants = None
+        if not (args.no_variants or world > 1):
+            nvtx.range_push("variants")
+            variants = run_variants(D, A, dA, Bt, dev, peak)
+            nvtx.range_pop()
         mixed = None if args.no_mixed else run_mixed(D, A, dA, B, dev, K, peak)
         if mixed is not None and world == 1:
             mixed["random_1m_deg8"] = run_mixed_random(D, dev, peak)
@@ -379,12 +409,18 @@ def run_ours(args):
         serving = None if (args.no_serving or world > 1) else run_serving(D, dev, args.serve_seconds)
         clk = sampler.summary()
         clk_in = sampler.summary(t0, t1)
-        clocks = {"sm_mhz": clk_in["sm_mhz"] if clk_in["samples"] else clk["sm_mhz"],
+        clk_sus = sampler.summary(t_s0, t_s1)
+        clocks = {"sm_mhz": clk_in["sm_mhz"] if clk_in["samples"] else clk_sus["sm_mhz"],
                   "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
-                  "samples_timed": clk_in["samples"], "samples_total": clk["samples"],
-                  "window": "200 ms nvidia-smi samples over a 1.5 s burst of the same step "
-                            "right before the timed region and the timed region itself"}
+                  "samples_timed": clk_in["samples"], "samples_sustained": clk_sus["samples"],
+                  "samples_total": clk["samples"],
+                  "window": "200 ms nvidia-smi samples from just before the timed region "
+                            "through the >= 1.2 s of the same step right after it (the "
+                            "timed region alone is shorter than one sample)"}
         cfg_used = D.default_config(alg, 0, A.nr, A.nc, A.nnz, NV)
+        if step_cfg is not None:
+            cfg_used.lanes_col = args.lanes_col or cfg_used.lanes_col
+            cfg_used.chunk = args.chunk or cfg_used.chunk
         line = {
             "metric": METRIC, "value": round(gflops, 3), "unit": UNIT, "n_gpus": world,
             "steps": K, "warmup": args.warmup, "ms_per_step": round(ms_step, 5),
@@ -395,13 +431,19 @@ def run_ours(args):
             "variant": dict(cfg_used.as_dict(), alg_name=alg.name),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4),
-                         "traffic": traffic, "kernel": "k_bal_half (main gather; timed with k_partition and the k_bal_lean list walk)",
+                         "traffic": traffic, "kernel": "k_bal_grp<16,8,8,float,float> (the main gather; CUDA events around each "
+                                   "launch of it in a second pass of K calls)",
                          "kernel_ms": round(kern_ms, 5), "algorithmic_bytes": abytes,
                          "gather_upper_bound_bytes": gather_bytes(A, NV),
                          "peak_source": peak_src},
             "step_hbm_gbs": round(abytes / (ms_step * 1e-3) / 1e9, 1),
+            "sustained": {"ms_per_step": round(sus_ms, 5), "steps": n_sus,
+                          "value": round(2.0 * nnz_total * NV / (sus_ms * 1e-3) / 1e9, 3),
+                          "sm_mhz": clk_sus["sm_mhz"],
+                          "what": "the same step back to back for >= 1.2 s right after the "
+                                  "timed region (power-capped clocks), rank 0"},
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": int(launches),
-            "reference_kernels": refk, "cusparse": cus, "variants": variants,
+            "plan": plan, "l2_window": l2win, "reference_kernels": refk, "cusparse": cus, "variants": variants,
             "mixed": mixed, "batched": batched, "serving": serving,
         }
     if pg:
@@ -410,6 +452,48 @@ def run_ours(args):
     if line is not None:
         print(json.dumps(line), flush=True)
     return 0
+
+
+def run_plan(D, A, dA, Bt, dev, peak, K):
+    """The same product through a plan (daspmm_plan_*): the balanced split's
+    boundaries computed once, each step one window-kernel launch (plus the
+    walk over listed chunks, none on this matrix).  K steps back to back
+    between CUDA events, after 5 warm-up steps; the result is compared bit for
+    bit with the stateless call's."""
+    import torch
+    L = D.lib()
+    plan = D.Plan(dA, NV)
+    Cp = torch.empty(A.nr * NV, device=dev)
+    Cs = torch.empty(A.nr * NV, device=dev)
+    for _ in range(5):
+        plan.spmm(Bt, Cp)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(K):
+        plan.spmm(Bt, Cp)
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / K
+    D.check(L.daspmm_kernel_timer_begin(K), "kernel_timer_begin")
+    for _ in range(K):
+        plan.spmm(Bt, Cp)
+    torch.cuda.synchronize(dev)
+    kt = (ctypes.c_float * K)()
+    n = L.daspmm_kernel_timer_end(kt, K)
+    kms = sum(kt) / max(1, n)
+    D.spmm(D.Alg.CSR_BALANCED, 0, dA, Bt, Cs, nv=NV, cfg=plan.config())
+    torch.cuda.synchronize(dev)
+    same = bool(torch.equal(Cp, Cs))
+    plan.close()
+    abytes = algorithmic_bytes(A, NV)
+    return {"value": round(2.0 * A.nnz * NV / (ms * 1e-3) / 1e9, 3), "unit": UNIT,
+            "ms_per_step": round(ms, 5), "step_frac": round(abytes / (ms * 1e-3) / 1e9 / peak, 4),
+            "kernel_ms": round(kms, 5),
+            "kernel_frac": round(abytes / (kms * 1e-3) / 1e9 / peak, 4),
+            "bit_identical_to_stateless": same,
+            "what": "daspmm_plan_spmm: boundaries computed once at plan creation; per step the "
+                    "window kernel and the walk over listed chunks"}
 
 
 REF_VARIANTS = [  # run.sh:29 column order: alg (spmvspmm.h:5-10) x layout
@@ -460,6 +544,39 @@ def run_reference_kernels(A, dA, Bt, dev, ours_ms, warmup=3, reps=20):
     cus["daspmm_speedup_vs_best"] = round(cus[bestc]["us"] / (ours_ms * 1e3), 3)
     del C
     return kern, cus
+
+
+def run_l2_window(D, A, dA, Bt, dev, peak, K=20):
+    """The default call with an L2 access-policy window over B (config
+    l2_window: thousandths of B's lines persisting) and a persisting L2
+    set-aside of the given size; K calls back to back between CUDA events.
+    The set-aside is reset to 0 afterwards."""
+    import torch
+    L = D.lib()
+    C = torch.zeros(A.nr * NV, device=dev)
+    abytes = algorithmic_bytes(A, NV)
+    out = {"set_aside": "MB requested (the library clamps to the device's largest)"}
+    try:
+        for mb, w in ((0, 0), (32, 250), (32, 1000), (64, 500), (64, 1000), (96, 1000)):
+            D.check(L.daspmm_l2_set_aside(mb << 20), "l2_set_aside")
+            cfg = D.Config(alg=4, l2_window=w)
+            run = lambda: D.spmm(D.Alg.CSR_BALANCED, 0, dA, Bt, C, nv=NV, cfg=cfg)
+            for _ in range(5):
+                run()
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(K):
+                run()
+            e1.record()
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / K
+            out[f"set_aside_{mb}MB_window_{w}"] = {
+                "us": round(ms * 1e3, 2),
+                "frac": round(abytes / (ms * 1e-3) / 1e9 / peak, 4)}
+    finally:
+        L.daspmm_l2_set_aside(0)
+    return out
 
 
 def run_variants(D, A, dA, Bt, dev, peak, K=20):
@@ -788,29 +905,36 @@ def run_serving(D, dev, seconds: float = 1.0, rate: float = 20000.0):
                        "plain_fp32_gflops": cap_p["gflops"],
                        "batched_mean_group": cap_b["mean_group"],
                        "ratio": round(cap_b["req_s"] / max(cap_p["req_s"], 1e-9), 3)}
-    # throughput at equal p99: the plain path at half its capacity sets the bound
-    half = 0.5 * cap_p["req_s"]
-    plain_half = run(P_, half)
-    bound = plain_half["p99_us"]
-    keeps_up = lambda q, r: q["p99_us"] <= bound and q["req_s"] >= 0.97 * r
-    lo, hi = half, 4.0 * cap_b["req_s"]
-    best = run(B_, lo)
-    if keeps_up(best, lo):
-        for _ in range(6):
-            mid = 0.5 * (lo + hi)
-            q = run(B_, mid)
-            if keeps_up(q, mid):
-                lo, best = mid, q
-            else:
-                hi = mid
-    out["equal_p99"] = {"p99_bound_us": bound, "plain_req_s": plain_half["req_s"],
-                        "plain_p99_us": plain_half["p99_us"],
-                        "batched_req_s": best["req_s"], "batched_p99_us": best["p99_us"],
-                        "batched_offered_req_s": best["offered_req_s"],
-                        "ratio": round(best["req_s"] / max(plain_half["req_s"], 1e-9), 3),
-                        "rule": "bound = plain FP32 p99 at half its capacity; batched: the "
-                                "highest offered Poisson rate (bisection) whose p99 stays "
-                                "within the bound and whose throughput keeps up (>= 97%)"}
+    # Throughput at equal p99.  The bound is the plain path's own p99 at a
+    # fraction f of its capacity (so the plain throughput at that bound is f x
+    # its capacity); the batched mode's throughput at the bound is its highest
+    # offered Poisson rate that keeps up (>= 97 %) within that p99, found by
+    # bisection between f x the plain capacity and 2 x its own capacity.
+    keeps_up = lambda q, r, b: q["p99_us"] <= b and q["req_s"] >= 0.97 * r
+    eq = []
+    for f in (0.5, 0.75, 0.9):
+        rp_ = f * cap_p["req_s"]
+        plain_f = run(P_, rp_)
+        bound = plain_f["p99_us"]
+        lo, hi = rp_, 2.0 * cap_b["req_s"]
+        best = run(B_, lo)
+        if keeps_up(best, lo, bound):
+            for _ in range(5):
+                mid = 0.5 * (lo + hi)
+                q = run(B_, mid)
+                if keeps_up(q, mid, bound):
+                    lo, best = mid, q
+                else:
+                    hi = mid
+        eq.append({"plain_load_fraction": f, "p99_bound_us": bound,
+                   "plain_req_s": plain_f["req_s"], "batched_req_s": best["req_s"],
+                   "batched_p99_us": best["p99_us"],
+                   "ratio": round(best["req_s"] / max(plain_f["req_s"], 1e-9), 3)})
+    out["equal_p99"] = {"points": eq,
+                        "rule": "bound = plain FP32 p99 at the given fraction of its capacity; "
+                                "batched: the highest offered Poisson rate (bisection) whose "
+                                "p99 stays within the bound and whose throughput keeps up "
+                                "(>= 97%)"}
     out["sweep"] = {"batched_bf16": [run(B_, r) for r in (10e3, 20e3, 40e3, 60e3, 80e3)],
                     "plain_fp32": [run(P_, r) for r in (5e3, 10e3, 15e3, 20e3)]}
     hot = 0.9 * cap_b["req_s"]
@@ -885,6 +1009,9 @@ def main():
     ap.add_argument("--alg", default="CSR_BALANCED",
                     choices=["CSR_SCALAR", "CSR_VECTOR", "COO_SCALAR", "COO_VECTOR",
                              "CSR_BALANCED", "AUTO"])
+    ap.add_argument("--lanes-col", type=int, default=0,
+                    help="CSR_BALANCED column tile: 32 (128 columns), 16 (64), 8 (32); 0 = default")
+    ap.add_argument("--chunk", type=int, default=0, help="nonzeros per chunk; 0 = default")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")

@@ -108,6 +108,8 @@ daspmm_status resolve(const daspmm_config *cfg, int layout, int nr, int nc, int 
     r.nc = nc;
     r.nnz = nnz;
     if (cfg->pipe < 0 || cfg->pipe > 5) return DASPMM_ERR_INVALID;
+    if (cfg->l2_window < 0 || cfg->l2_window > 1000) return DASPMM_ERR_INVALID;
+    r.l2_window = cfg->l2_window;
     if (cfg->pipe == 5 && !(r.cm && cfg->alg == DASPMM_ALG_CSR_BALANCED))
         return DASPMM_ERR_UNSUPPORTED;
     // Column-major balanced CSR with 4 or more columns: transpose B to
@@ -305,10 +307,9 @@ static void launch_all(const Resolved &r, KArgs &a, dim3 grid, dim3 fix_grid, in
                        cudaStream_t st)
 {
     const bool fix = a.nchunks > 1;
-    // the lean pair's timing starts before k_partition (run_resolved), so no
-    // event sits between kernels that overlap by programmatic launch
-    const bool lean = r.alg == DASPMM_ALG_CSR_BALANCED && r.pipe == 4;
-    if (!lean) timer_before(st);
+    // the main kernel (pipe 4: the window or walk kernel after k_partition)
+    // sits between the optional timer events
+    timer_before(st);
     switch (r.alg) {
     case DASPMM_ALG_CSR_SCALAR:
     case DASPMM_ALG_CSR_VECTOR:
@@ -411,6 +412,8 @@ daspmm_status run_resolved(const Resolved &r, int layout, int nr, int nc, int nn
     a.rowPtr = rowPtr; a.rowIdx = rowIdx; a.colIdx = colIdx; a.vals = values;
     a.B = B; a.C = C; a.beta = beta;
     a.L = r.L; a.S = r.S; a.chunk = r.chunk; a.nchunks = r.nchunks;
+    a.l2_window = r.l2_window;
+    a.b_bytes = sizeof(float) * (size_t)nc * nv;
     const int G = r.L * r.S;
 
     if (coo) {
@@ -428,7 +431,6 @@ daspmm_status run_resolved(const Resolved &r, int layout, int nr, int nc, int nn
         a.slots = (float *)ws;
     } else if (r.alg == DASPMM_ALG_CSR_BALANCED) {
         carve_balanced(r, ws, &a);
-        if (r.pipe == 4) timer_before(st);
         launch_partition(r, nr, nnz, rowPtr, a, st);
     }
     const long long units =
@@ -439,6 +441,52 @@ daspmm_status run_resolved(const Resolved &r, int layout, int nr, int nc, int nn
     if (s != DASPMM_OK) return s;
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? DASPMM_OK : cuda_fail(e);
+}
+
+bool run_planned(const Resolved &r, int nr, int nc, int nnz, int nv, const int *rowPtr,
+                 const int *colIdx, const float *values, const float *B, float *C, void *ws,
+                 unsigned long long call, cudaStream_t st)
+{
+    if (r.alg != DASPMM_ALG_CSR_BALANCED || r.cm || r.pipe != 4 || nr <= 0) return false;
+    // chunks per group of the window kernel: 32 / (W / 8) workers per warp
+    const int nw = r.W == 128 ? 2 : 4;
+    const unsigned long long ngroups = ((unsigned long long)r.nchunks + nw - 1) / nw;
+    KArgs a{};
+    a.nr = nr; a.nc = nc; a.nnz = nnz; a.nv = nv;
+    a.ldb = nv; a.ldc = nv;
+    a.rowPtr = rowPtr; a.colIdx = colIdx; a.vals = values;
+    a.B = B; a.C = C; a.beta = 0.0f;
+    a.L = r.L; a.S = r.S; a.chunk = r.chunk; a.nchunks = r.nchunks;
+    a.l2_window = r.l2_window;
+    a.b_bytes = sizeof(float) * (size_t)nc * nv;
+    a.list_mode = 2;  // the plan's fixed list of chunks with an empty row
+    a.head_base = (unsigned int)(call * ngroups);  // claims of the calls before, mod 2^32
+    carve_balanced(r, ws, &a);
+    timer_before(st);
+    bool ok = false;
+    if (r.W == 128 && (ok = launch_grp<128, float, float>(r, a, st)))
+        launch_walk_list<128, float, float>(r, a, st);
+    else if (r.W == 64 && (ok = launch_grp<64, float, float>(r, a, st)))
+        launch_walk_list<64, float, float>(r, a, st);
+    timer_after(st);
+    if (ok) count_launches(1);
+    return ok;
+}
+
+void workspace_tables(const Resolved &r, void *ws, const int2 **meta, int **list)
+{
+    KArgs a{};
+    carve_balanced(r, ws, &a);
+    *meta = a.meta;
+    *list = a.list;
+}
+
+void carve_and_partition(const Resolved &r, int nr, int nnz, const int *rowPtr, void *ws,
+                         cudaStream_t st)
+{
+    KArgs a{};
+    carve_balanced(r, ws, &a);
+    launch_partition(r, nr, nnz, rowPtr, a, st);
 }
 
 void carve_balanced(const Resolved &r, void *ws, KArgs *a)
@@ -711,6 +759,19 @@ daspmm_status daspmm_wait_probe(int polls, int expire, int *out, void *stream)
     k_wait_probe<<<1, 32, 0, (cudaStream_t)stream>>>(polls, expire ? 1 : 0, out);
     count_launches(1);
     cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? DASPMM_OK : cuda_fail(e);
+}
+
+daspmm_status daspmm_l2_set_aside(size_t bytes)
+{
+    int dev = 0, maxp = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&maxp, cudaDevAttrMaxPersistingL2CacheSize, dev);
+    if (e != cudaSuccess) return cuda_fail(e);
+    if (bytes > (size_t)maxp) bytes = (size_t)maxp;  // the device's largest set-aside
+    e = cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, bytes);
+    if (e == cudaSuccess && bytes == 0) e = cudaCtxResetPersistingL2Cache();
     return e == cudaSuccess ? DASPMM_OK : cuda_fail(e);
 }
 

@@ -146,147 +146,174 @@ __device__ __forceinline__ float ld_val(const T *p, uint64_t pol)
 #define DASPMM_LEAN_U 4     // nonzeros (B rows) in flight per warp step
 #endif
 
-template <int W, int U, typename TV = float, typename TB = float, bool KAHAN = false>
-__global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_lean(const KArgs a)
+// One chunk of the balanced split, column tile `tile` of `tiles`, summed by
+// the whole warp with the per-nonzero walk: every nonzero is compared with
+// the end of the current row (row ends from a 32-entry lane cache), so empty
+// rows, beta != 0 and Kahan rows are all handled.  A row split across chunks
+// leaves its pieces in carry slots; the last piece to arrive adds them all
+// in chunk order (piece_arrive).  W / 32 elements of the B row per lane.
+template <int W, int U, typename TV, typename TB, bool KAHAN>
+__device__ __forceinline__ void lean_chunk(const KArgs &a, int c, int tile, int tiles,
+                                           uint64_t pol_once)
 {
     constexpr int VL = W / 32;  // elements of the B row per lane
     constexpr bool SCALED = std::is_same<TB, fp8>::value;
     const int lane = threadIdx.x & 31;
-    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    const int tb = blockIdx.y * W + lane * VL;
+    const int tb = tile * W + lane * VL;
     const TB *Bl = reinterpret_cast<const TB *>(a.B) + tb;
     const TV *Av = reinterpret_cast<const TV *>(a.vals);
-    const uint64_t pol_once = policy_evict_first();
-    pdl_wait();  // the boundaries (k_partition) or the list (k_bal_fast) are complete
-    float sc[VL];  // read after the wait, like every input
+    float sc[VL];
 #pragma unroll
     for (int e = 0; e < VL; ++e) sc[e] = SCALED ? __ldg(a.bscale + tb + e) : 1.0f;
+    const int2 m0 = a.meta[c], m1 = a.meta[c + 1];
+    const int k0 = m0.x, k1 = m1.x, s1 = m1.y;
+    int r = m0.y;
+    bool cont = k0 > __ldg(a.rowPtr + r);
+    // row-end cache: lane l holds rowPtr[rb + 1 + l]; the next 32 are prefetched
+    int rb = r;
+    int rc = __ldg(a.rowPtr + min(rb + 1 + lane, a.nr));
+    int rn = __ldg(a.rowPtr + min(rb + 33 + lane, a.nr));
+    int re = __shfl_sync(kFull, rc, 0);
+    float acc[VL], comp[VL];
+#pragma unroll
+    for (int e = 0; e < VL; ++e) acc[e] = comp[e] = 0.0f;
+    // Kahan rows: length of the current row (its start is the previous end)
+    int rs = KAHAN ? __ldg(a.rowPtr + r) : 0;
+    bool kh = KAHAN && re - rs >= a.kahan_min;
+
+    const bool head_piece = cont;  // row m0.y continues from an earlier chunk
+    auto emit = [&](int row, bool ends) {
+        if constexpr (SCALED) {
+#pragma unroll
+            for (int e = 0; e < VL; ++e) acc[e] *= sc[e];
+        }
+        if (ends && !cont) {
+            float *dst = a.C + (size_t)row * a.ldc + tb;
+            if (a.beta != 0.0f) {
+                float old[VL];
+                ld_plain<VL>(old, dst);
+#pragma unroll
+                for (int e = 0; e < VL; ++e) acc[e] = fmaf(a.beta, old[e], acc[e]);
+            }
+            st_hint<VL>(dst, acc, pol_once);
+        } else {  // a piece of a row split across chunks: park it in its carry slot
+            st_v<VL>(slot_ptr(a, c, cont ? 0 : 1, tb), acc);
+        }
+#pragma unroll
+        for (int e = 0; e < VL; ++e) acc[e] = comp[e] = 0.0f;
+        cont = false;
+    };
+    auto step = [&](int p, float v, const float (&b)[VL]) {
+        while (p >= re) {
+            emit(r, true);
+            ++r;
+            if (r - rb >= 32) {
+                rb += 32;
+                rc = rn;
+                rn = __ldg(a.rowPtr + min(rb + 33 + lane, a.nr));
+            }
+            if constexpr (KAHAN) rs = re;
+            re = __shfl_sync(kFull, rc, r - rb);
+            if constexpr (KAHAN) kh = re - rs >= a.kahan_min;
+        }
+        if (KAHAN && kh) {
+#pragma unroll
+            for (int e = 0; e < VL; ++e) {  // Kahan: carry the rounding error along
+                const float y = fmaf(v, b[e], -comp[e]);
+                const float t = acc[e] + y;
+                comp[e] = (t - acc[e]) - y;
+                acc[e] = t;
+            }
+        } else {
+#pragma unroll
+            for (int e = 0; e < VL; ++e) acc[e] = fmaf(v, b[e], acc[e]);
+        }
+    };
+    // Windows of 32 nonzeros: lane l holds the column/value of nonzero
+    // wb + l; the next window's are loaded while this one is gathered.
+    auto load_win = [&](int wb, int &col, float &val) {
+        const bool ok = wb + lane < k1;
+        col = ok ? ld_hint_s32(a.colIdx + wb + lane, pol_once) : 0;
+        val = ok ? ld_val<TV>(Av + wb + lane, pol_once) : 0.0f;
+    };
+    int ccur, cnext;
+    float vcur, vnext;
+    load_win(k0, ccur, vcur);
+    for (int wb = k0; wb < k1; wb += 32) {
+        load_win(wb + 32, cnext, vnext);
+        const int cnt = min(32, k1 - wb);
+        int t = 0;
+        for (; t + U <= cnt; t += U) {  // U rows in flight
+            int cc[U];
+            float vv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                cc[u] = __shfl_sync(kFull, ccur, t + u);
+                vv[u] = __shfl_sync(kFull, vcur, t + u);
+            }
+            float b[U][VL];
+#pragma unroll
+            for (int u = 0; u < U; ++u) ld_b<TB, VL>(b[u], Bl + (size_t)cc[u] * a.ldb);
+#pragma unroll
+            for (int u = 0; u < U; ++u) step(wb + t + u, vv[u], b[u]);
+        }
+        for (; t < cnt; ++t) {
+            float b[VL];
+            ld_b<TB, VL>(b, Bl + (size_t)__shfl_sync(kFull, ccur, t) * a.ldb);
+            step(wb + t, __shfl_sync(kFull, vcur, t), b);
+        }
+        ccur = cnext;
+        vcur = vnext;
+    }
+    while (r < s1) {
+        emit(r, true);
+        ++r;
+    }
+    const int head_row = m0.y;
+    bool tail_piece = false;
+    if (r < a.nr && r == s1 && __ldg(a.rowPtr + r) < k1) {
+        tail_piece = !cont;  // a continuing row here is the head piece itself
+        emit(r, false);
+    }
+    // the pieces this chunk parked arrive (at most two; fence + count, and
+    // the last piece of a row adds them all)
+    if (head_piece) piece_arrive<VL>(a, head_row, tb, tiles, tile);
+    if (tail_piece) piece_arrive<VL>(a, s1, tb, tiles, tile);
+}
+
+template <int W, int U, typename TV = float, typename TB = float, bool KAHAN = false>
+__global__ void __launch_bounds__(256, DASPMM_LEAN_MINB) k_bal_lean(const KArgs a)
+{
+    const int lane = threadIdx.x & 31;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const uint64_t pol_once = policy_evict_first();
+    pdl_wait();  // the boundaries (k_partition) or the list (k_bal_fast) are complete
     // Queue mode: chunks are handed out dynamically -- each warp starts with
     // chunk = its index, then takes the next unclaimed one from the column
     // tile's queue head (zeroed by k_partition), so warps that draw short
     // chunks take more and no wave of chunks is left half-used.  List mode:
     // the chunks k_bal_fast left over (a.list), strided over the warps.
+    // Plan mode (2): the list is the planned product's fixed list of chunks
+    // with an empty row, unless row 0 of B holds an Inf or NaN -- then the
+    // window kernel took no chunk and every chunk is walked here.
     const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const long long limit = a.list_mode ? (long long)a.list[0] : (long long)a.nchunks;
+    bool all = false;
+    if (a.list_mode == 2) {
+        bool pad_ok = true;
+        for (int k = lane; a.nnz > 0 && k < a.nv; k += 32) {
+            float x[1];
+            ld_b<TB, 1>(x, reinterpret_cast<const TB *>(a.B) + k);
+            pad_ok &= isfinite(x[0]);
+        }
+        all = !__all_sync(kFull, pad_ok);
+    }
+    const long long limit = (a.list_mode && !all) ? (long long)a.list[0] : (long long)a.nchunks;
     long long cl = wid;
     while (cl < limit) {
-        const int c = a.list_mode ? a.list[1 + cl] : (int)cl;
-        const int2 m0 = a.meta[c], m1 = a.meta[c + 1];
-        const int k0 = m0.x, k1 = m1.x, s1 = m1.y;
-        int r = m0.y;
-        bool cont = k0 > __ldg(a.rowPtr + r);
-        // row-end cache: lane l holds rowPtr[rb + 1 + l]; the next 32 are prefetched
-        int rb = r;
-        int rc = __ldg(a.rowPtr + min(rb + 1 + lane, a.nr));
-        int rn = __ldg(a.rowPtr + min(rb + 33 + lane, a.nr));
-        int re = __shfl_sync(kFull, rc, 0);
-        float acc[VL], comp[VL];
-#pragma unroll
-        for (int e = 0; e < VL; ++e) acc[e] = comp[e] = 0.0f;
-        // Kahan rows: length of the current row (its start is the previous end)
-        int rs = KAHAN ? __ldg(a.rowPtr + r) : 0;
-        bool kh = KAHAN && re - rs >= a.kahan_min;
-
-        const bool head_piece = cont;  // row m0.y continues from an earlier chunk
-        auto emit = [&](int row, bool ends) {
-            if constexpr (SCALED) {
-#pragma unroll
-                for (int e = 0; e < VL; ++e) acc[e] *= sc[e];
-            }
-            if (ends && !cont) {
-                float *dst = a.C + (size_t)row * a.ldc + tb;
-                if (a.beta != 0.0f) {
-                    float old[VL];
-                    ld_plain<VL>(old, dst);
-#pragma unroll
-                    for (int e = 0; e < VL; ++e) acc[e] = fmaf(a.beta, old[e], acc[e]);
-                }
-                st_hint<VL>(dst, acc, pol_once);
-            } else {  // a piece of a row split across chunks: park it in its carry slot
-                st_v<VL>(slot_ptr(a, c, cont ? 0 : 1, tb), acc);
-            }
-#pragma unroll
-            for (int e = 0; e < VL; ++e) acc[e] = comp[e] = 0.0f;
-            cont = false;
-        };
-        auto step = [&](int p, float v, const float (&b)[VL]) {
-            while (p >= re) {
-                emit(r, true);
-                ++r;
-                if (r - rb >= 32) {
-                    rb += 32;
-                    rc = rn;
-                    rn = __ldg(a.rowPtr + min(rb + 33 + lane, a.nr));
-                }
-                if constexpr (KAHAN) rs = re;
-                re = __shfl_sync(kFull, rc, r - rb);
-                if constexpr (KAHAN) kh = re - rs >= a.kahan_min;
-            }
-            if (KAHAN && kh) {
-#pragma unroll
-                for (int e = 0; e < VL; ++e) {  // Kahan: carry the rounding error along
-                    const float y = fmaf(v, b[e], -comp[e]);
-                    const float t = acc[e] + y;
-                    comp[e] = (t - acc[e]) - y;
-                    acc[e] = t;
-                }
-            } else {
-#pragma unroll
-                for (int e = 0; e < VL; ++e) acc[e] = fmaf(v, b[e], acc[e]);
-            }
-        };
-        // Windows of 32 nonzeros: lane l holds the column/value of nonzero
-        // wb + l; the next window's are loaded while this one is gathered.
-        auto load_win = [&](int wb, int &col, float &val) {
-            const bool ok = wb + lane < k1;
-            col = ok ? ld_hint_s32(a.colIdx + wb + lane, pol_once) : 0;
-            val = ok ? ld_val<TV>(Av + wb + lane, pol_once) : 0.0f;
-        };
-        int ccur, cnext;
-        float vcur, vnext;
-        load_win(k0, ccur, vcur);
-        for (int wb = k0; wb < k1; wb += 32) {
-            load_win(wb + 32, cnext, vnext);
-            const int cnt = min(32, k1 - wb);
-            int t = 0;
-            for (; t + U <= cnt; t += U) {  // U rows in flight
-                int cc[U];
-                float vv[U];
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    cc[u] = __shfl_sync(kFull, ccur, t + u);
-                    vv[u] = __shfl_sync(kFull, vcur, t + u);
-                }
-                float b[U][VL];
-#pragma unroll
-                for (int u = 0; u < U; ++u) ld_b<TB, VL>(b[u], Bl + (size_t)cc[u] * a.ldb);
-#pragma unroll
-                for (int u = 0; u < U; ++u) step(wb + t + u, vv[u], b[u]);
-            }
-            for (; t < cnt; ++t) {
-                float b[VL];
-                ld_b<TB, VL>(b, Bl + (size_t)__shfl_sync(kFull, ccur, t) * a.ldb);
-                step(wb + t, __shfl_sync(kFull, vcur, t), b);
-            }
-            ccur = cnext;
-            vcur = vnext;
-        }
-        while (r < s1) {
-            emit(r, true);
-            ++r;
-        }
-        const int head_row = m0.y;
-        bool tail_piece = false;
-        if (r < a.nr && r == s1 && __ldg(a.rowPtr + r) < k1) {
-            tail_piece = !cont;  // a continuing row here is the head piece itself
-            emit(r, false);
-        }
-        // the pieces this chunk parked arrive (at most two; fence + count, and
-        // the last piece of a row adds them all)
-        if (head_piece) piece_arrive<VL>(a, head_row, tb, gridDim.y, blockIdx.y);
-        if (tail_piece) piece_arrive<VL>(a, s1, tb, gridDim.y, blockIdx.y);
+        const int c = (a.list_mode && !all) ? a.list[1 + cl] : (int)cl;
+        lean_chunk<W, U, TV, TB, KAHAN>(a, c, blockIdx.y, gridDim.y, pol_once);
         if (a.list_mode) {
-            cl += nwarps;
+            cl += nwarps;  // listed chunks (or, plan mode with a non-finite row 0, all)
         } else {
             unsigned int nx = 0;
             if (lane == 0) nx = atomicAdd(a.head + blockIdx.y, 1u);
@@ -546,6 +573,8 @@ static __device__ __noinline__ void piece_arrive_grp(const int *__restrict__ row
     if ((threadIdx.x & (G - 1)) == 0) last = atomicAdd(cnt + (size_t)c0 * tiles + tile, 1) == c1 - c0;
     last = __shfl_sync(gmask, last, 0, G);
     if (!last) return;
+    // every piece has arrived: the counter goes back to zero for the next call
+    if ((threadIdx.x & (G - 1)) == 0) cnt[(size_t)c0 * tiles + tile] = 0;
     __threadfence();
     float tot[VL];
     ld_cg_n<VL>(tot, slots + ((size_t)c0 * 2 + 1) * nv + col);
@@ -663,7 +692,8 @@ __global__ void __launch_bounds__(256, DASPMM_GRP_MINB) k_bal_grp(const KArgs a)
             }
         }
         const bool skip = !have || empty_row || !pad_ok;
-        if (have && (empty_row || !pad_ok) && tile == 0 && gl == 0)
+        // the walk kernel sums these; a planned product's list is fixed
+        if (have && (empty_row || !pad_ok) && tile == 0 && gl == 0 && a.list_mode != 2)
             a.list[1 + atomicAdd(a.list, 1)] = c;  // every tile
         const int kb = skip ? 0 : k0, ke = skip ? 0 : k1;
         int nwin = (ke - kb + G - 1) / G;
@@ -745,86 +775,121 @@ __global__ void __launch_bounds__(256, DASPMM_GRP_MINB) k_bal_grp(const KArgs a)
             piece_arrive_grp<G, EPL, TV, TB>(a.rowPtr, a.cnt, a.slots, a.C, a.ldc, a.nv, a.chunk,
                                              s1, tb, tiles, tile, gmask);
         __syncwarp();
+        // the next group from the tile's queue; a call makes exactly ngroups
+        // claims, so a planned product counts on from where the last one ended
         unsigned int nx = 0;
-        if (lane == 0) nx = atomicAdd(a.head + tile, 1u);
+        if (lane == 0) nx = atomicAdd(a.head + tile, 1u) - a.head_base;
         gi = nwarps + (long long)__shfl_sync(kFull, nx, 0);
     }
 }
 
-// The lean pair: for beta == 0 without Kahan rows, k_bal_fast over every
-// chunk and k_bal_lean over the chunks it listed; otherwise k_bal_lean over
-// every chunk.  Grids: the CTAs that fit at once (chunks are handed out by
-// the queue), and one CTA per SM for the listed chunks.
 // A launch that may overlap the previous kernel of the stream (programmatic
 // dependent launch); the kernel calls pdl_wait() before reading its inputs.
+// With a.l2_window > 0 the launch also carries an L2 access-policy window
+// over B (that many thousandths of its lines persisting, the rest streaming).
 // A failure is left in the runtime's last error for the caller's check.
-template <typename... P>
-inline void launch_pdl(void (*kernel)(P...), dim3 grid, cudaStream_t st, P... args)
+inline void launch_pdl(void (*kernel)(KArgs), dim3 grid, cudaStream_t st, const KArgs &a)
 {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = dim3(256);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = st;
-    cudaLaunchAttribute at[1];
+    cudaLaunchAttribute at[2];
     at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     at[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = at;
     cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, kernel, args...);
+    if (a.l2_window > 0 && a.b_bytes > 0) {
+        int dev = 0, maxw = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxAccessPolicyWindowSize, dev);
+        at[1].id = cudaLaunchAttributeAccessPolicyWindow;
+        at[1].val.accessPolicyWindow.base_ptr = const_cast<float *>(a.B);
+        at[1].val.accessPolicyWindow.num_bytes = std::min<size_t>(a.b_bytes, (size_t)maxw);
+        at[1].val.accessPolicyWindow.hitRatio = std::min(1.0f, a.l2_window / 1000.0f);
+        at[1].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+        at[1].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+        cfg.numAttrs = maxw > 0 ? 2 : 1;
+    }
+    cfg.attrs = at;
+    cudaLaunchKernelEx(&cfg, kernel, a);
 }
 
+// The worker-group kernel, when it takes this product: beta == 0, EPL
+// elements of B per lane load (FP32: 8 in 32 bytes; BF16 / FP16: 16 in 32
+// bytes; E4M3: 16 in 16 bytes), G = W / EPL lanes per chunk, stores of C and
+// carries 32-byte aligned.  Returns false (nothing launched) otherwise.
+// Measured on the 262k power-law matrix: the group form wins for FP32 storage
+// and 128- or 64-column tiles (N = 128: 84 against 113 us, N = 64: 54 against
+// 61 us); for 32-column FP32 tiles (G = 4) the 32-lane kernel is as fast or
+// faster (41 against 42 us at N = 32).  BF16 / FP16 / E4M3 B: the group form
+// wins from two 128-column tiles on (BF16 N = 256: 155 against 173 us, N =
+// 512: 282 against 335; E4M3 N = 512: 239 against 318), the 32-lane kernel
+// for one (BF16 N = 128: 77 against 84 us; E4M3 equal).
+template <int W, typename TV, typename TB>
+inline bool launch_grp(const Resolved &r, const KArgs &a, cudaStream_t st)
+{
+    constexpr bool f32 = std::is_same<TV, float>::value && std::is_same<TB, float>::value;
+    constexpr int EPL = std::is_same<TB, float>::value ? 8 : 16;
+    constexpr int G = W / EPL;
+    constexpr bool grp_ok = f32 ? W >= 64 : W == 128;
+    if constexpr (!grp_ok) {
+        return false;
+    } else {
+        const bool aligned_g =
+            (reinterpret_cast<uintptr_t>(a.B) % (EPL * sizeof(TB))) == 0 &&
+            ((reinterpret_cast<uintptr_t>(a.C) | reinterpret_cast<uintptr_t>(a.slots)) % 32) ==
+                0 &&
+            a.ldb % EPL == 0 && a.ldc % 8 == 0 && a.nv % W == 0;
+        if (!(DASPMM_GRP && a.beta == 0.0f && aligned_g && (f32 || r.tiles >= 2))) return false;
+        constexpr int NWK = 32 / G;
+        const long long groups = ((long long)a.nchunks + NWK - 1) / NWK;
+        const unsigned gg = (unsigned)std::max<long long>(
+            1, std::min<long long>((groups + 7) / 8, (long long)device_sms() * DASPMM_GRP_MINB));
+        launch_pdl(k_bal_grp<G, EPL, f32 ? DASPMM_GRP_U : DASPMM_GRP_U16, TV, TB>,
+                   dim3(gg, r.tiles), st, a);
+        return true;
+    }
+}
+
+// The walk kernel over the chunks the window kernel listed (list mode).
+template <int W, typename TV, typename TB>
+inline void launch_walk_list(const Resolved &r, KArgs a, cudaStream_t st)
+{
+    const long long resident = (long long)device_sms() * DASPMM_LEAN_MINB;
+    const unsigned gx = (unsigned)std::max<long long>(
+        1, std::min<long long>(((long long)a.nchunks + 7) / 8, resident));
+    if (a.list_mode != 2) a.list_mode = 1;
+    const unsigned gw = std::min<unsigned>(gx, (unsigned)device_sms());
+    launch_pdl(k_bal_lean<W, DASPMM_LEAN_U, TV, TB, false>, dim3(gw, r.tiles), st, a);
+    count_launches(1);
+}
+
+// The lean pair: for beta == 0 without Kahan rows, the window kernel (the
+// worker-group form where it takes the product, else k_bal_fast) over every
+// chunk and k_bal_lean over the chunks it listed; otherwise k_bal_lean over
+// every chunk.  Grids: the CTAs that fit at once (chunks are handed out by
+// the queue), and one CTA per SM for the listed chunks.
 template <int W, typename TV, typename TB, bool K>
 inline void launch_lean(const Resolved &r, KArgs a, cudaStream_t st)
 {
     const long long resident = (long long)device_sms() * DASPMM_LEAN_MINB;
     const unsigned gx = (unsigned)std::max<long long>(
         1, std::min<long long>(((long long)a.nchunks + 7) / 8, resident));
+    a.list_mode = 0;
     if (!K && a.beta == 0.0f) {
-        a.list_mode = 0;
-        // the worker-group kernel: EPL elements of B per lane load (FP32: 8 in
-        // 32 bytes; BF16 / FP16: 16 in 32 bytes; E4M3: 16 in 16 bytes),
-        // G = W / EPL lanes per chunk; stores of C and carries 32-byte aligned
-        constexpr bool f32 = std::is_same<TV, float>::value && std::is_same<TB, float>::value;
-        constexpr int EPL = std::is_same<TB, float>::value ? 8 : 16;
-        constexpr int G = W / EPL;
-        const bool aligned_g =
-            (reinterpret_cast<uintptr_t>(a.B) % (EPL * sizeof(TB))) == 0 &&
-            ((reinterpret_cast<uintptr_t>(a.C) | reinterpret_cast<uintptr_t>(a.slots)) % 32) ==
-                0 &&
-            a.ldb % EPL == 0 && a.ldc % 8 == 0 && a.nv % W == 0;
-        // measured on the 262k power-law matrix: the group form wins for FP32
-        // storage and 128- or 64-column tiles (N = 128: 84 against 113 us,
-        // N = 64: 54 against 61 us); for 32-column FP32 tiles (G = 4) the
-        // 32-lane kernel is as fast or faster (41 against 42 us at N = 32).
-        // BF16 / FP16 / E4M3 B: the group form wins from two 128-column tiles
-        // on (BF16 N = 256: 155 against 173 us, N = 512: 282 against 335;
-        // E4M3 N = 512: 239 against 318), the 32-lane kernel for one (BF16
-        // N = 128: 77 against 84 us; E4M3 equal).
-        constexpr bool grp_ok = f32 ? W >= 64 : W == 128;
-        if (grp_ok && DASPMM_GRP && aligned_g && (f32 || r.tiles >= 2)) {
-            constexpr int NWK = 32 / (grp_ok ? G : 32);
-            const long long groups = ((long long)a.nchunks + NWK - 1) / NWK;
-            const unsigned gg = (unsigned)std::max<long long>(
-                1, std::min<long long>((groups + 7) / 8,
-                                       (long long)device_sms() * DASPMM_GRP_MINB));
-            if constexpr (grp_ok)
-                launch_pdl(k_bal_grp<G, EPL, f32 ? DASPMM_GRP_U : DASPMM_GRP_U16, TV, TB>,
-                           dim3(gg, r.tiles), st, a);
-        } else if constexpr (W == 128) {
-            launch_pdl(k_bal_fast<W, DASPMM_LEAN_U, TV, TB>, dim3(gx, r.tiles), st, a);
-        } else {  // one queue of (tile, chunk) items
-            const long long items = (long long)a.nchunks * r.tiles;
-            const unsigned gi = (unsigned)std::max<long long>(
-                1, std::min<long long>((items + 7) / 8, resident));
-            launch_pdl(k_bal_fast<W, DASPMM_LEAN_U, TV, TB>, dim3(gi), st, a);
+        if (!launch_grp<W, TV, TB>(r, a, st)) {
+            if constexpr (W == 128) {
+                launch_pdl(k_bal_fast<W, DASPMM_LEAN_U, TV, TB>, dim3(gx, r.tiles), st, a);
+            } else {  // one queue of (tile, chunk) items
+                const long long items = (long long)a.nchunks * r.tiles;
+                const unsigned gi = (unsigned)std::max<long long>(
+                    1, std::min<long long>((items + 7) / 8, resident));
+                launch_pdl(k_bal_fast<W, DASPMM_LEAN_U, TV, TB>, dim3(gi), st, a);
+            }
         }
-        a.list_mode = 1;
-        const unsigned gw = std::min<unsigned>(gx, (unsigned)device_sms());
-        launch_pdl(k_bal_lean<W, DASPMM_LEAN_U, TV, TB, K>, dim3(gw, r.tiles), st, a);
-        count_launches(1);
+        launch_walk_list<W, TV, TB>(r, a, st);
     } else {
-        a.list_mode = 0;
         launch_pdl(k_bal_lean<W, DASPMM_LEAN_U, TV, TB, K>, dim3(gx, r.tiles), st, a);
     }
 }

@@ -23,6 +23,7 @@ struct Resolved {
                // gather, 5 column-major through a row-major product (transposes)
     int W;     // TMA ring: tile width in floats (32, 64, 128)
     int inner_chunk;  // pipe 5: the caller's chunk for the row-major product
+    int l2_window;    // thousandths of B's lines marked L2-persisting (0 = off)
 };
 
 // SMs of the current device (148 when no device is visible).
@@ -42,6 +43,7 @@ inline daspmm_config to_config(const Resolved &r)
     c.snap = r.snap;
     c.block = r.block;
     c.pipe = r.pipe;
+    c.l2_window = r.l2_window;
     return c;
 }
 
@@ -61,7 +63,24 @@ struct KArgs;
 void carve_balanced(const Resolved &r, void *ws, KArgs *a);
 void launch_partition(const Resolved &r, int nr, int nnz, const int *rowPtr, const KArgs &a,
                       cudaStream_t st);
+// carve_balanced + launch_partition on a workspace (the boundaries and the
+// zeroed queue state of the balanced split).
+void carve_and_partition(const Resolved &r, int nr, int nnz, const int *rowPtr, void *ws,
+                         cudaStream_t st);
 daspmm_status cached_workspace(size_t need, cudaStream_t st, void **out);
+// A planned FP32 row-major balanced-CSR product (plan.cu): the worker-group
+// window kernel alone, over a workspace whose chunk boundaries k_partition
+// wrote once (the kernel leaves its queue heads and split-row counters at
+// zero).  Returns false, launching nothing, when that kernel does not take
+// the call (beta != 0, alignment, tile width).
+// `call` counts the planned products since the boundaries were computed: a
+// call's window kernel makes exactly one queue claim per chunk group, so
+// each call counts its claims on from call x groups (no reset between calls).
+bool run_planned(const Resolved &r, int nr, int nc, int nnz, int nv, const int *rowPtr,
+                 const int *colIdx, const float *values, const float *B, float *C, void *ws,
+                 unsigned long long call, cudaStream_t st);
+// The boundary table and the walk list inside a balanced-CSR workspace.
+void workspace_tables(const Resolved &r, void *ws, const int2 **meta, int **list);
 daspmm_status cached_host_staging(size_t need, cudaStream_t st, void **out);
 
 // Launch accounting and the optional event hook around main kernels.

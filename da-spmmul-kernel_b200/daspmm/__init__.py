@@ -62,7 +62,8 @@ class Config(ctypes.Structure):
     """daspmm_config: one point of the design space (0 = library default)."""
 
     _fields_ = [(n, ctypes.c_int) for n in
-                ("alg", "vec", "lanes_col", "lanes_nnz", "cf", "chunk", "snap", "block", "pipe")]
+                ("alg", "vec", "lanes_col", "lanes_nnz", "cf", "chunk", "snap", "block", "pipe",
+                 "l2_window")]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}
@@ -363,6 +364,41 @@ def fingerprint(layout: int, A: DeviceCsr, nv: int, dtype: int = 0, stream=None)
 
 
 # ---------------------------------------------------------------- batches
+class Plan:
+    """daspmm_plan_*: one matrix (a DeviceCsr that must outlive the plan), row-
+    major, nv columns; the balanced split's boundaries computed once, each
+    product one launch of the window kernel (bit-identical to spmm with the
+    same configuration)."""
+
+    def __init__(self, A: DeviceCsr, nv: int, cfg: Config | None = None, stream=None):
+        self.A, self.nv = A, int(nv)
+        self._h = ctypes.c_void_p()
+        check(_lib().daspmm_plan_create(ctypes.byref(cfg) if cfg is not None else None, A.nr,
+                                        A.nc, A.nnz, self.nv, _dptr(A.rowPtr), _dptr(A.colIdx),
+                                        _dptr(A.values), _stream_ptr(stream),
+                                        ctypes.byref(self._h)), "plan_create")
+
+    def spmm(self, B, C, beta: float = 0.0, stream=None) -> None:
+        check(_lib().daspmm_plan_spmm(self._h, _dptr(B), _dptr(C), float(beta),
+                                      _stream_ptr(stream)), "plan_spmm")
+
+    def config(self) -> Config:
+        c = Config()
+        check(_lib().daspmm_plan_config(self._h, ctypes.byref(c)), "plan_config")
+        return c
+
+    def close(self):
+        if self._h:
+            _lib().daspmm_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Batch:
     """Many SpMMs in one persistent launch (daspmm_batch_*).
 

@@ -88,6 +88,11 @@ def apply(lib, Config):
         "daspmm_e4m3_scales": (_I, [_I, _I, _VP, _VP, _VP]),
         "daspmm_device_error": (_I, []),
         "daspmm_wait_probe": (_I, [_I, _I, _VP, _VP]),
+        "daspmm_plan_create": (_I, [_VP, _I, _I, _I, _I, _VP, _VP, _VP, _VP, _VP]),
+        "daspmm_plan_spmm": (_I, [_VP, _VP, _VP, ctypes.c_float, _VP]),
+        "daspmm_plan_config": (_I, [_VP, _VP]),
+        "daspmm_plan_destroy": (_I, [_VP]),
+        "daspmm_l2_set_aside": (_I, [ctypes.c_size_t]),
         "daspmm_mtx_info": (_I, [ctypes.c_char_p, ctypes.POINTER(MtxHeader)]),
         "daspmm_mtx_read": (_I, [ctypes.c_char_p, _I, _LL, _VP, _VP, _VP, _VP,
                                  ctypes.POINTER(_I)]),

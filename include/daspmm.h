@@ -29,7 +29,7 @@ extern "C" {
 #pragma GCC visibility push(default)
 #endif
 
-#define DASPMM_ABI_VERSION 1
+#define DASPMM_ABI_VERSION 2
 
 typedef enum daspmm_status {
     DASPMM_OK = 0,
@@ -81,6 +81,12 @@ typedef struct daspmm_config {
                        row-major product, C transposed back (the default from
                        nv >= 4; A read once for all columns).
                        0 = the library's choice */
+    int l2_window;  /* balanced CSR, row-major window and walk kernels: 0 = off;
+                       1..1000 = an L2 access-policy window over B on the main
+                       kernel's launch, that many thousandths of its lines
+                       marked persisting (the rest streaming).  Has an effect
+                       only with a persisting L2 set-aside
+                       (daspmm_l2_set_aside).  Results do not depend on it. */
 } daspmm_config;
 
 /* ---- FP32 SpMM ---------------------------------------------------------
@@ -406,6 +412,30 @@ daspmm_status daspmm_spmm_host_async(const daspmm_config *cfg, int layout, int n
                                      const int *colIdx, const float *values, const float *B,
                                      float *C, float beta, void *stream);
 
+/* ---- Planned SpMM: one matrix, many products ---------------------------
+ * No counterpart in the reference (its benchmark loop, spmvspmm.h:220-243,
+ * times one problem; its kernels need no partition).  daspmm_spmm recomputes
+ * the balanced split's chunk boundaries (a pass over rowPtr) in every call,
+ * so the matrix may change between calls.  A plan fixes the matrix (device
+ * rowPtr / colIdx / values, which must stay unchanged and alive until
+ * daspmm_plan_destroy), row-major layout and nv: the boundaries are computed
+ * once, into a workspace the plan owns, and each daspmm_plan_spmm with beta
+ * == 0 and B / C 32-byte aligned is one launch of the window kernel.  Results
+ * are bit-identical to daspmm_spmm with the plan's configuration.  Other calls
+ * (beta != 0, other alignment) take the stateless path on the plan's
+ * workspace.  cfg: NULL or {.alg = DASPMM_ALG_CSR_BALANCED, ...}.
+ * daspmm_plan_create allocates (cudaMalloc) and synchronises `stream`.
+ * Calls on one plan share its workspace: order them (one stream); calls that
+ * overlap on the GPU race. */
+typedef struct daspmm_plan_s *daspmm_plan;
+daspmm_status daspmm_plan_create(const daspmm_config *cfg, int nr, int nc, int nnz, int nv,
+                                 const int *rowPtr, const int *colIdx, const float *values,
+                                 void *stream, daspmm_plan *out);
+daspmm_status daspmm_plan_spmm(daspmm_plan p, const float *B, float *C, float beta,
+                               void *stream);
+daspmm_status daspmm_plan_config(daspmm_plan p, daspmm_config *out);
+daspmm_status daspmm_plan_destroy(daspmm_plan p);
+
 /* ---- No device allocation ----------------------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc
  * -- a plugin inside an application whose own allocator owns the device's
@@ -441,6 +471,17 @@ daspmm_status daspmm_spmm_noalloc(int layout, int nr, int nc, int nnz, int nv,
                                   const int *rowPtr, const int *colIdx,
                                   const float *values, const float *B, float *C,
                                   float beta, void *stream);
+
+/* ---- L2 persistence ---------------------------------------------------
+ * No counterpart in the reference.  Sets the current device's persisting L2
+ * set-aside (cudaLimitPersistingL2CacheSize) for this process's context, used
+ * by launches whose config has l2_window > 0, at most the device's largest
+ * (cudaDevAttrMaxPersistingL2CacheSize; larger requests are clamped to it);
+ * 0 resets it and returns the persisting lines to normal
+ * (cudaCtxResetPersistingL2Cache).  The setting is
+ * the context's: it ends with the process and applies to all of its work on
+ * the device. */
+daspmm_status daspmm_l2_set_aside(size_t bytes);
 
 /* ---- Diagnostics ------------------------------------------------------- */
 /* Reads and clears the device-side error word of the current device: 0, or

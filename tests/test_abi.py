@@ -36,7 +36,7 @@ def test_every_declared_symbol_is_exported():
 
 def test_abi_version_and_status_strings():
     L = D.lib()
-    assert L.daspmm_abi_version() == 1
+    assert L.daspmm_abi_version() == 2
     for s in range(10):
         assert L.daspmm_status_string(s)
     assert L.daspmm_status_string(0) == b"ok"

@@ -253,6 +253,43 @@ def test_no_columns_no_nonzeros(cuda):
                     assert torch.all(C == 2.0 * beta), f"{alg.name} layout {layout} nv {nv}"
 
 
+def test_l2_window_knob(cuda):
+    """An L2 access-policy window over B (config l2_window, with a persisting
+    set-aside) changes where B's lines live in L2, not the arithmetic: the
+    products are bit-identical with and without it, FP32 and BF16 storage."""
+    import torch
+    L = D.lib()
+    A = D.gen_powerlaw(20000, dmax=2000, seed=8)
+    dA = D.DeviceCsr(A)
+    rng = np.random.default_rng(8)
+    try:
+        assert L.daspmm_l2_set_aside(32 << 20) == 0
+        for nv in (64, 128, 256):
+            B = rng.uniform(-1, 1, A.nc * nv).astype(np.float32)
+            Bt = torch.from_numpy(B).cuda()
+            ref = torch.empty(A.nr * nv, device="cuda")
+            D.spmm(D.Alg.CSR_BALANCED, 0, dA, Bt, ref, nv=nv, cfg=D.Config(alg=4))
+            b16 = D.quantize(Bt, D.Fmt.BF16)
+            v16 = D.quantize(dA.values, D.Fmt.BF16)
+            ref16 = torch.empty(A.nr * nv, device="cuda")
+            D.spmm_mixed(dA, v16, D.Fmt.BF16, b16, D.Fmt.BF16, ref16, nv)
+            for w in (250, 1000):
+                C = torch.full((A.nr * nv,), float("nan"), device="cuda")
+                D.spmm(D.Alg.CSR_BALANCED, 0, dA, Bt, C, nv=nv, cfg=D.Config(alg=4, l2_window=w))
+                C16 = torch.full((A.nr * nv,), float("nan"), device="cuda")
+                D.spmm_mixed(dA, v16, D.Fmt.BF16, b16, D.Fmt.BF16, C16, nv,
+                             cfg=D.Config(alg=4, l2_window=w))
+                torch.cuda.synchronize()
+                assert torch.equal(C, ref), f"nv={nv} window {w}"
+                assert torch.equal(C16, ref16), f"BF16 nv={nv} window {w}"
+            _check(A, 0, nv, B, ref.cpu().numpy(), what=f"l2 window nv={nv}")
+        bad = torch.empty(A.nr * 64, device="cuda")
+        with pytest.raises(D.DaspmmError):
+            D.spmm(D.Alg.CSR_BALANCED, 0, dA, Bt, bad, nv=64, cfg=D.Config(alg=4, l2_window=1001))
+    finally:
+        assert L.daspmm_l2_set_aside(0) == 0
+
+
 def test_partition_bit_exact(mats):
     for name in ("uniform", "powerlaw", "random", "hub"):
         A, dA = mats[name]
