@@ -772,8 +772,10 @@ def run_batched(D, dev, reps: int = 20):
                          B=D.quantize(B32, D.Fmt.BF16), b_fmt=D.Fmt.BF16, C=C))
         plain.append((dA, B32, torch.zeros_like(C)))
     total_nnz = sum(A.nnz for A in mats)
-    chunk, _ = D.Batch.tune(inst, chunks=[128, 256, 512, 1024], reps=3)
-    batch = D.Batch(inst, chunk=chunk)
+    # row-tile size and column-tile width tuned together (N = 64: tiles of 64 or 32 floats)
+    best, _ = D.Batch.tune_ex(inst, chunks=[128, 256, 512, 1024], widths=[64, 32], reps=3)
+    chunk = best.chunk
+    batch = D.Batch(inst, chunk=chunk, lanes_col=best.lanes_col)
     s = torch.cuda.Stream(dev)
     batch.capture(s)
     for _ in range(3):
@@ -818,7 +820,8 @@ def run_batched(D, dev, reps: int = 20):
     batch.close()
     flop = 2.0 * total_nnz * nv
     return {"instances": len(mats), "total_nnz": total_nnz, "nv": nv, "items": items,
-            "chunk_autotuned": chunk, "storage": "FP32 values, BF16 B, FP32 accumulate",
+            "chunk_autotuned": chunk, "tile_width_autotuned": 4 * best.lanes_col,
+            "storage": "FP32 values, BF16 B, FP32 accumulate",
             "value": round(flop / (ms_b * 1e-3) / 1e9, 3), "unit": UNIT, "ms_per_batch": round(ms_b, 4),
             "plain_fp32_one_launch_per_instance": {"value": round(flop / (ms_p * 1e-3) / 1e9, 3),
                                                    "ms_per_batch": round(ms_p, 4)},

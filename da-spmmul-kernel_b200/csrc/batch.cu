@@ -377,10 +377,12 @@ bool batch_formats_ok(int vf, int bf)
            (vf == DASPMM_BF16 && bf == DASPMM_E4M3);
 }
 
-daspmm_status batch_fill(const daspmm_instance &s, BatchInst *d)
+daspmm_status batch_fill(const daspmm_instance &s, BatchInst *d, int wcap)
 {
     if (s.nv < 1 || s.nr < 0 || s.nc < 0 || s.nnz < 0) return DASPMM_ERR_INVALID;
-    const int W = batch_tile_width(s.nv), VL = W / 32;
+    int W = batch_tile_width(s.nv);
+    if (wcap == 32 || wcap == 64) W = std::min(W, wcap);  // narrower column tiles
+    const int VL = W / 32;
     if (s.nv % VL != 0 || (s.nr > 0 && (!s.rowPtr || !s.C)) ||
         (s.nnz > 0 && (!s.colIdx || !s.values || !s.B)) ||
         (s.b_fmt == DASPMM_E4M3 && s.nr > 0 && !s.b_scales) ||
@@ -534,6 +536,13 @@ daspmm_status daspmm_batch_create(const daspmm_instance *inst, int n, const dasp
     cudaGetDevice(&b->device);
     b->ninst = n;
     b->chunk = (cfg && cfg->chunk > 0) ? cfg->chunk : 256;
+    // lanes_col 16 / 8: column tiles of at most 64 / 32 floats (0, 32: the
+    // widest of 128 / 64 / 32 dividing the instance's nv)
+    const int wcap = (cfg && (cfg->lanes_col == 8 || cfg->lanes_col == 16)) ? 4 * cfg->lanes_col : 0;
+    if (cfg && cfg->lanes_col && cfg->lanes_col != 8 && cfg->lanes_col != 16 && cfg->lanes_col != 32) {
+        delete b;
+        return DASPMM_ERR_INVALID;
+    }
     if (n > 0) {
         b->nv = inst[0].nv;
         b->val_fmt = inst[0].val_fmt;
@@ -548,7 +557,7 @@ daspmm_status daspmm_batch_create(const daspmm_instance *inst, int n, const dasp
         const daspmm_instance &s = inst[i];
         const daspmm_status fs = (s.val_fmt != b->val_fmt || s.b_fmt != b->b_fmt)
                                      ? DASPMM_ERR_INVALID
-                                     : batch_fill(s, &hi[i]);
+                                     : batch_fill(s, &hi[i], wcap);
         if (fs != DASPMM_OK) {
             delete b;
             return fs;
@@ -688,9 +697,14 @@ daspmm_status daspmm_batch_info(daspmm_batch b, long long *nitems, long long *to
     return DASPMM_OK;
 }
 
-daspmm_status daspmm_batch_tune(const daspmm_instance *inst, int n, const int *chunks,
-                                int nchunks, int reps, int *best_chunk, float *best_us,
-                                void *stream)
+}  // extern "C"
+
+namespace daspmm {
+// The fastest of `chunks` for these instances at the column-tile setting of
+// `base` (lanes_col), each timed over `reps` runs after two warm-ups.
+daspmm_status batch_tune_chunks(const daspmm_instance *inst, int n, const int *chunks,
+                                int nchunks, daspmm_config base, int reps, int *best_chunk,
+                                float *best_us, void *stream)
 {
     static const int kDefault[] = {128, 256, 512, 1024};
     if (!chunks || nchunks <= 0) {
@@ -703,7 +717,7 @@ daspmm_status daspmm_batch_tune(const daspmm_instance *inst, int n, const int *c
     float bus = 0.0f;
     int bch = 0;
     for (int k = 0; k < nchunks; ++k) {
-        daspmm_config cfg{};
+        daspmm_config cfg = base;
         cfg.chunk = chunks[k];
         daspmm_batch b = nullptr;
         daspmm_status s = daspmm_batch_create(inst, n, &cfg, &b, stream);
@@ -730,6 +744,57 @@ daspmm_status daspmm_batch_tune(const daspmm_instance *inst, int n, const int *c
         }
     }
     *best_chunk = bch;
+    if (best_us) *best_us = bus;
+    return DASPMM_OK;
+}
+}  // namespace daspmm
+
+extern "C" {
+
+daspmm_status daspmm_batch_tune(const daspmm_instance *inst, int n, const int *chunks,
+                                int nchunks, int reps, int *best_chunk, float *best_us,
+                                void *stream)
+{
+    if (!best_chunk) return DASPMM_ERR_INVALID;
+    return batch_tune_chunks(inst, n, chunks, nchunks, daspmm_config{}, reps, best_chunk,
+                             best_us, stream);
+}
+
+daspmm_status daspmm_batch_tune_ex(const daspmm_instance *inst, int n, const int *chunks,
+                                   int nchunks, const int *widths, int nwidths, int reps,
+                                   daspmm_config *best, float *best_us, void *stream)
+{
+    static const int kChunks[] = {128, 256, 512, 1024};
+    static const int kWidths[] = {128, 64, 32};
+    if (!chunks || nchunks <= 0) {
+        chunks = kChunks;
+        nchunks = 4;
+    }
+    if (!widths || nwidths <= 0) {
+        widths = kWidths;
+        nwidths = 3;
+    }
+    if (!best || reps < 0) return DASPMM_ERR_INVALID;
+    for (int w = 0; w < nwidths; ++w)
+        if (widths[w] != 32 && widths[w] != 64 && widths[w] != 128) return DASPMM_ERR_INVALID;
+    float bus = 0.0f;
+    bool have = false;
+    daspmm_config bc{};
+    for (int w = 0; w < nwidths; ++w) {
+        int ch = 0;
+        float us = 0.0f;
+        daspmm_config c{};
+        c.lanes_col = widths[w] / 4;
+        daspmm_status s = batch_tune_chunks(inst, n, chunks, nchunks, c, reps, &ch, &us, stream);
+        if (s != DASPMM_OK) return s;
+        if (!have || us < bus) {
+            have = true;
+            bus = us;
+            bc = c;
+            bc.chunk = ch;
+        }
+    }
+    *best = bc;
     if (best_us) *best_us = bus;
     return DASPMM_OK;
 }

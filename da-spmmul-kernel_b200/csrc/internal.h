@@ -144,7 +144,10 @@ int batch_tile_width(int nv);
 bool batch_formats_ok(int val_fmt, int b_fmt);
 // Checks one instance and fills its kernel-side row except tiles / ntiles /
 // slots / cnt (DASPMM_ERR_INVALID on a bad size, pointer or alignment).
-daspmm_status batch_fill(const daspmm_instance &s, BatchInst *d);
+daspmm_status batch_fill(const daspmm_instance &s, BatchInst *d, int wcap = 0);
+daspmm_status batch_tune_chunks(const daspmm_instance *inst, int n, const int *chunks,
+                                int nchunks, daspmm_config base, int reps, int *best_chunk,
+                                float *best_us, void *stream);
 // item table of n instances whose item counts (ntiles * col_tiles) prefix to
 // d_begin[0..n].
 daspmm_status batch_plan_async(const BatchInst *d_inst, const long long *d_begin, int n,

@@ -109,9 +109,10 @@ daspmm_status fingerprint(int layout, int nr, int nnz, int nv, int dtype, const 
 std::vector<daspmm_config> candidates(int layout, int nv, bool have_coo)
 {
     std::vector<daspmm_config> v;
-    auto add = [&](int alg, int pipe = 0, int chunk = 0, int S = 0, int cf = 0) {
+    auto add = [&](int alg, int pipe = 0, int chunk = 0, int S = 0, int cf = 0, int L = 0) {
         daspmm_config c{};
         c.alg = alg; c.pipe = pipe; c.chunk = chunk; c.lanes_nnz = S; c.cf = cf;
+        c.lanes_col = L;
         v.push_back(c);
     };
     add(DASPMM_ALG_CSR_SCALAR);
@@ -121,7 +122,12 @@ std::vector<daspmm_config> candidates(int layout, int nv, bool have_coo)
         add(DASPMM_ALG_COO_VECTOR);
     }
     if (layout == DASPMM_ROW_MAJOR && nv % 32 == 0) {
-        for (int ch : {64, 128, 256}) add(DASPMM_ALG_CSR_BALANCED, 4, ch);
+        // the window kernel: chunk sizes at the widest tile, then narrower
+        // column tiles (64 / 32 floats: G = 8 / the 32-lane kernel)
+        for (int ch : {64, 96, 128, 256}) add(DASPMM_ALG_CSR_BALANCED, 4, ch);
+        for (int L : {16, 8})
+            if (nv % (4 * L) == 0 && (nv % 128 == 0 || (L == 8 && nv % 64 == 0)))
+                for (int ch : {64, 128}) add(DASPMM_ALG_CSR_BALANCED, 4, ch, 0, 0, L);
         add(DASPMM_ALG_CSR_BALANCED, 3);
         add(DASPMM_ALG_CSR_BALANCED, 2);
         add(DASPMM_ALG_CSR_BALANCED, 1);

@@ -406,7 +406,7 @@ class Batch:
     tensor, F32 or BF16), B, C (device tensors), nv, optional val_fmt, b_fmt,
     b_scales, beta.  The tensors must outlive the batch."""
 
-    def __init__(self, instances, chunk: int = 0, stream=None):
+    def __init__(self, instances, chunk: int = 0, stream=None, lanes_col: int = 0):
         from ._sigs import Instance
         self._keep = instances
         arr = (Instance * max(1, len(instances)))()
@@ -418,7 +418,7 @@ class Batch:
                               int(d.get("b_fmt", Fmt.F32)), _dptr(d.get("b_scales")) or 0,
                               _dptr(d["C"]) or 0, float(d.get("beta", 0.0)))
         self._h = ctypes.c_void_p()
-        cfg = Config(chunk=chunk)
+        cfg = Config(chunk=chunk, lanes_col=lanes_col)
         check(_lib().daspmm_batch_create(arr, len(instances), ctypes.byref(cfg),
                                          ctypes.byref(self._h), _stream_ptr(stream)),
               "batch_create")
@@ -450,6 +450,28 @@ class Batch:
                                        reps, ctypes.byref(best), ctypes.byref(us),
                                        _stream_ptr(stream)), "batch_tune")
         return best.value, us.value
+
+    @staticmethod
+    def tune_ex(instances, chunks=None, widths=None, reps: int = 5, stream=None):
+        """Fastest (row-tile size, column-tile width) for these instances:
+        (Config with chunk and lanes_col, us)."""
+        from ._sigs import Instance
+        arr = (Instance * max(1, len(instances)))()
+        for i, d in enumerate(instances):
+            A = d["A"]
+            arr[i] = Instance(A.nr, A.nc, A.nnz, d["nv"], _dptr(A.rowPtr) or 0,
+                              _dptr(A.colIdx) or 0, _dptr(d.get("values", A.values)) or 0,
+                              int(d.get("val_fmt", Fmt.F32)), _dptr(d["B"]) or 0,
+                              int(d.get("b_fmt", Fmt.F32)), _dptr(d.get("b_scales")) or 0,
+                              _dptr(d["C"]) or 0, float(d.get("beta", 0.0)))
+        ch = (ctypes.c_int * len(chunks))(*chunks) if chunks else None
+        wd = (ctypes.c_int * len(widths))(*widths) if widths else None
+        best, us = Config(), ctypes.c_float()
+        check(_lib().daspmm_batch_tune_ex(arr, len(instances), ch, len(chunks) if chunks else 0,
+                                          wd, len(widths) if widths else 0, reps,
+                                          ctypes.byref(best), ctypes.byref(us),
+                                          _stream_ptr(stream)), "batch_tune_ex")
+        return best, us.value
 
     def info(self):
         a, b = ctypes.c_longlong(), ctypes.c_longlong()

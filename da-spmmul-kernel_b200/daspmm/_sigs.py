@@ -93,6 +93,7 @@ def apply(lib, Config):
         "daspmm_plan_config": (_I, [_VP, _VP]),
         "daspmm_plan_destroy": (_I, [_VP]),
         "daspmm_l2_set_aside": (_I, [ctypes.c_size_t]),
+        "daspmm_batch_tune_ex": (_I, [_VP, _I, _VP, _I, _VP, _I, _I, _VP, _VP, _VP]),
         "daspmm_mtx_info": (_I, [ctypes.c_char_p, ctypes.POINTER(MtxHeader)]),
         "daspmm_mtx_read": (_I, [ctypes.c_char_p, _I, _LL, _VP, _VP, _VP, _VP,
                                  ctypes.POINTER(_I)]),

@@ -262,6 +262,16 @@ daspmm_status daspmm_batch_destroy(daspmm_batch b);
 daspmm_status daspmm_batch_tune(const daspmm_instance *inst, int n, const int *chunks,
                                 int nchunks, int reps, int *best_chunk, float *best_us,
                                 void *stream);
+/* No counterpart in the reference.  Tunes the row-tile size and the column-
+ * tile width together: for every width in `widths` (floats: 128, 64 or 32;
+ * NULL = all three; an instance's tile is the widest of 128 / 64 / 32 that
+ * divides its nv and is at most the width) the fastest of `chunks` (NULL =
+ * 128, 256, 512, 1024), each batch timed over `reps` runs.  *best receives
+ * the winning daspmm_batch_create config (chunk, lanes_col = width / 4).
+ * Results do not depend on either choice. */
+daspmm_status daspmm_batch_tune_ex(const daspmm_instance *inst, int n, const int *chunks,
+                                   int nchunks, const int *widths, int nwidths, int reps,
+                                   daspmm_config *best, float *best_us, void *stream);
 
 /* ---- Matrix Market input ---------------------------------------------------
  * Coordinate files (real, integer or pattern values; general, symmetric,

@@ -173,3 +173,36 @@ def test_batch_tune_and_autotuner(cuda, tmp_path):
         or cfg.alg == 4
     assert D.lib().daspmm_tune_load(path.encode()) == 0
     assert D.default_config(D.Alg.AUTO, 0, A.nr, A.nc, A.nnz, 128).as_dict() == cfg.as_dict()
+
+
+def test_batch_tile_width_and_joint_tuner(cuda):
+    """Narrower column tiles (lanes_col 16 / 8: at most 64 / 32 floats) give
+    bit-identical results (each output element is summed in the same order
+    whatever the tile), and the joint row-tile / column-tile tuner returns one
+    of its candidates."""
+    import torch
+    rng = np.random.default_rng(11)
+    nv = 128
+    mats = _instances(rng, nv, n=12)
+    for vf, bf in ((D.Fmt.F32, D.Fmt.F32), (D.Fmt.F32, D.Fmt.BF16)):
+        inst = _prepare(mats, nv, vf, bf, rng)
+        ref = None
+        for lanes in (0, 16, 8):
+            for d in inst:
+                d["C"].fill_(float("nan"))
+            b = D.Batch(inst, chunk=256, lanes_col=lanes)
+            b.run()
+            torch.cuda.synchronize()
+            out = [d["C"].clone() for d in inst]
+            b.close()
+            if ref is None:
+                ref = out
+                for d in inst:
+                    _check(d)
+            else:
+                for r, o in zip(ref, out):
+                    assert torch.equal(r, o), f"lanes_col {lanes} differs"
+        best, us = D.Batch.tune_ex(inst, chunks=[128, 512], widths=[128, 64], reps=2)
+        assert best.chunk in (128, 512) and best.lanes_col in (32, 16) and us > 0
+    with pytest.raises(D.DaspmmError):
+        D.Batch(inst, lanes_col=4)
