@@ -536,6 +536,25 @@ __device__ __forceinline__ void ld_raw(uint32_t (&w)[NW], const void *p)
         w[0] = t.x; w[1] = t.y; w[2] = t.z; w[3] = t.w;
     }
 }
+// acc[0] += a * lo(w), acc[1] += a * hi(w) for two packed 16-bit B elements
+// and a 16-bit value a of the same type (BF16 or FP16), FP32 accumulate in one
+// instruction each (fma.rn.f32.bf16 / .f16, sm_100): the product of two 16-bit
+// values is exact in FP32, so each result is the single rounding of
+// a*b + acc -- bit-identical to fmaf on the widened operands.
+template <typename T>
+__device__ __forceinline__ void fma2_16(float &acc0, float &acc1, unsigned short a, uint32_t w)
+{
+    unsigned short lo, hi;
+    asm("mov.b32 {%0, %1}, %2;" : "=h"(lo), "=h"(hi) : "r"(w));
+    if constexpr (std::is_same<T, bf16>::value) {
+        asm("fma.rn.f32.bf16 %0, %1, %2, %0;" : "+f"(acc0) : "h"(a), "h"(lo));
+        asm("fma.rn.f32.bf16 %0, %1, %2, %0;" : "+f"(acc1) : "h"(a), "h"(hi));
+    } else {
+        asm("fma.rn.f32.f16 %0, %1, %2, %0;" : "+f"(acc0) : "h"(a), "h"(lo));
+        asm("fma.rn.f32.f16 %0, %1, %2, %0;" : "+f"(acc1) : "h"(a), "h"(hi));
+    }
+}
+
 template <typename TB, int NW>
 __device__ __forceinline__ float elem(const uint32_t (&w)[NW], int i)
 {
@@ -632,6 +651,10 @@ __global__ void __launch_bounds__(256, DASPMM_GRP_MINB) k_bal_grp(const KArgs a)
     constexpr int UU = U < G ? U : G;                      // rows in flight per step
     constexpr unsigned GM = G == 32 ? 0xFFFFFFFFu : ((1u << G) - 1u);
     constexpr bool SCALED = std::is_same<TB, fp8>::value;
+    // FP16 values and B: one mixed-precision FMA per element (measured 2-3%
+    // faster at N = 256 / 512; the BF16 form of that instruction measured
+    // slower than unpacking to FP32, so BF16 unpacks)
+    constexpr bool PAIR16 = std::is_same<TV, fp16>::value && std::is_same<TB, fp16>::value;
     const int lane = threadIdx.x & 31, w = lane / G, gl = lane % G;
     const unsigned gmask = GM << (G * w);
     const int tile = blockIdx.y, tiles = gridDim.y;
@@ -737,9 +760,17 @@ __global__ void __launch_bounds__(256, DASPMM_GRP_MINB) k_bal_grp(const KArgs a)
                 for (int u = 0; u < UU; ++u) ld_raw<RAW>(b[u], Bl + (size_t)cc[u] * a.ldb);
 #pragma unroll
                 for (int u = 0; u < UU; ++u) {
+                    if constexpr (PAIR16) {
+                        // vv holds the FP16 value widened exactly: narrowing is exact
+                        const unsigned short a16 = __half_as_ushort(__float2half_rn(vv[u]));
 #pragma unroll
-                    for (int e = 0; e < EPL; ++e)
-                        acc[e] = fmaf(vv[u], elem<TB, RAW>(b[u], e), acc[e]);
+                        for (int i = 0; i < RAW; ++i)
+                            fma2_16<TB>(acc[2 * i], acc[2 * i + 1], a16, b[u][i]);
+                    } else {
+#pragma unroll
+                        for (int e = 0; e < EPL; ++e)
+                            acc[e] = fmaf(vv[u], elem<TB, RAW>(b[u], e), acc[e]);
+                    }
                     if ((ends >> (g * UU + u)) & 1u) {
                         if constexpr (SCALED) {
 #pragma unroll
