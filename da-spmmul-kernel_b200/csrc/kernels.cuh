@@ -560,30 +560,32 @@ static __global__ void k_partition(int nr, int nnz, const int *__restrict__ rowP
     // launched as a programmatic dependent of the stream's previous kernel (the
     // last SpMM's walk, say): nothing is read or written before it completes
     asm volatile("griddepcontrol.wait;" ::: "memory");
-    const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (r == 0) {
+    const long long r0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r0 == 0) {
         meta[0] = make_int2(0, 0);
         meta[nchunks] = make_int2(nnz, nr);
         if (head)
             for (int t = 0; t < tiles; ++t) head[t] = 0;
         if (list) list[0] = 0;
     }
-    if (r >= nr) return;
-    const int rs = __ldg(rowPtr + r), re = __ldg(rowPtr + r + 1);
-    if (rs == re) return;
-    long long c = ((long long)rs + chunk - 1) / chunk;
-    if (c < 1) c = 1;
-    bool split = false;
-    for (; c < nchunks && c * chunk < re; ++c) {
-        const int k = (int)(c * chunk);
-        const int kk = (k > rs && re - rs < snap) ? rs : k;
-        meta[c] = make_int2(kk, (int)r);
-        split |= kk > rs;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long r = r0; r < nr; r += stride) {
+        const int rs = __ldg(rowPtr + r), re = __ldg(rowPtr + r + 1);
+        if (rs == re) continue;
+        long long c = ((long long)rs + chunk - 1) / chunk;
+        if (c < 1) c = 1;
+        bool split = false;
+        for (; c < nchunks && c * chunk < re; ++c) {
+            const int k = (int)(c * chunk);
+            const int kk = (k > rs && re - rs < snap) ? rs : k;
+            meta[c] = make_int2(kk, (int)r);
+            split |= kk > rs;
+        }
+        // a row split across chunks: its arrival counters (one per column
+        // tile) live at its first chunk
+        if (split && cnt)
+            for (int t = 0; t < tiles; ++t) cnt[(size_t)(rs / chunk) * tiles + t] = 0;
     }
-    // a row split across chunks: its arrival counters (one per column tile)
-    // live at its first chunk
-    if (split && cnt)
-        for (int t = 0; t < tiles; ++t) cnt[(size_t)(rs / chunk) * tiles + t] = 0;
 }
 
 // Chunks holding pieces of a split row r (rows >= snap long are cut only at
