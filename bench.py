@@ -664,7 +664,7 @@ def run_mixed(D, A, dA, B, dev, steps, peak):
     C = torch.zeros(A.nr * NV, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
     for name, vf, bf in (("f32", D.Fmt.F32, D.Fmt.F32), ("bf16", D.Fmt.BF16, D.Fmt.BF16),
-                         ("bf16_e4m3", D.Fmt.BF16, D.Fmt.E4M3)):
+                         ("f16", D.Fmt.F16, D.Fmt.F16), ("bf16_e4m3", D.Fmt.BF16, D.Fmt.E4M3)):
         vq = vt if vf == D.Fmt.F32 else D.quantize(vt, vf)
         scales = D.e4m3_scales(Bt, A.nc, NV) if bf == D.Fmt.E4M3 else None
         bq = Bt if bf == D.Fmt.F32 else D.quantize(Bt, bf, scales, NV if scales is not None else 0)
@@ -687,7 +687,7 @@ def run_mixed(D, A, dA, B, dev, steps, peak):
         ms = s.elapsed_time(e) / steps
         kms = sum(kt) / max(1, n)
         sv = 4 if vf == D.Fmt.F32 else 2
-        sb = {D.Fmt.F32: 4, D.Fmt.BF16: 2, D.Fmt.E4M3: 1}[bf]
+        sb = {D.Fmt.F32: 4, D.Fmt.BF16: 2, D.Fmt.F16: 2, D.Fmt.E4M3: 1}[bf]
         abytes = algorithmic_bytes(A, NV, s_val=sv, s_b=sb) + (4 * NV if sb == 1 else 0)
         out[name] = {"value": round(2.0 * A.nnz * NV / (ms * 1e-3) / 1e9, 3), "unit": UNIT,
                      "ms_per_step": round(ms, 5), "kernel_ms": round(kms, 5),
@@ -695,7 +695,7 @@ def run_mixed(D, A, dA, B, dev, steps, peak):
                      "roofline_frac": round(abytes / (kms * 1e-3) / 1e9 / peak, 4),
                      "err_vs_fp64": mixed_error(D, A, NV, Bt, vf, bf, vq, bq, scales, C)}
     out["speedup_vs_f32"] = {k: round(out["f32"]["ms_per_step"] / out[k]["ms_per_step"], 3)
-                             for k in ("bf16", "bf16_e4m3")}
+                             for k in ("bf16", "f16", "bf16_e4m3")}
     return out
 
 
@@ -713,11 +713,13 @@ def run_mixed_random(D, dev, peak, steps: int = 10):
     g = torch.Generator(device=dev)
     g.manual_seed(0)
     vq = D.quantize(dA.values, D.Fmt.BF16)
+    vh = D.quantize(dA.values, D.Fmt.F16)
     out = {"nr": A.nr, "nnz": A.nnz}
     for nv in (32, 128, 512):
         Bt = torch.empty(A.nc * nv, device=dev).uniform_(-1, 1, generator=g)
         C = torch.zeros(A.nr * nv, dtype=torch.float32, device=dev)
         b16 = D.quantize(Bt, D.Fmt.BF16)
+        bh = D.quantize(Bt, D.Fmt.F16)
         sc = D.e4m3_scales(Bt, A.nc, nv)
         b8 = D.quantize(Bt, D.Fmt.E4M3, sc, nv)
         runs = {
@@ -725,6 +727,8 @@ def run_mixed_random(D, dev, peak, steps: int = 10):
                     (D.Fmt.F32, D.Fmt.F32, dA.values, Bt, None)),
             "bf16": (lambda: D.spmm_mixed(dA, vq, D.Fmt.BF16, b16, D.Fmt.BF16, C, nv), 2, 2,
                      (D.Fmt.BF16, D.Fmt.BF16, vq, b16, None)),
+            "f16": (lambda: D.spmm_mixed(dA, vh, D.Fmt.F16, bh, D.Fmt.F16, C, nv), 2, 2,
+                    (D.Fmt.F16, D.Fmt.F16, vh, bh, None)),
             "bf16_e4m3": (lambda: D.spmm_mixed(dA, vq, D.Fmt.BF16, b8, D.Fmt.E4M3, C, nv,
                                                b_scales=sc), 2, 1,
                           (D.Fmt.BF16, D.Fmt.E4M3, vq, b8, sc)),
@@ -749,7 +753,7 @@ def run_mixed_random(D, dev, peak, steps: int = 10):
                          "gather_bound_frac": round(gbytes / (kms * 1e-3) / 1e9 / peak, 4),
                          "err_vs_fp64": mixed_error(D, A, nv, Bt, vf, bf, vv, bb, ss, C)}
         out[f"n{nv}"] = res
-        del Bt, C, b16, b8
+        del Bt, C, b16, bh, b8
     return out
 
 

@@ -619,7 +619,10 @@ static __device__ __noinline__ void piece_arrive_grp(const int *__restrict__ row
 #define DASPMM_GRP_U 8      // nonzeros in flight per worker step
 #endif
 #ifndef DASPMM_GRP_U16
-#define DASPMM_GRP_U16 8    // the same for 2- and 1-byte B (16 elements per lane load)
+#define DASPMM_GRP_U16 16   // 2-byte B (8 elements per 16-byte lane load)
+#endif
+#ifndef DASPMM_GRP_U8
+#define DASPMM_GRP_U8 8     // 1-byte B (16 elements per 16-byte lane load)
 #endif
 #ifndef DASPMM_GRP_MINB
 #define DASPMM_GRP_MINB 2   // CTAs of 256 threads per SM: 16 warps, <= 128 registers
@@ -847,22 +850,26 @@ inline void launch_pdl(void (*kernel)(KArgs), dim3 grid, cudaStream_t st, const 
 }
 
 // The worker-group kernel, when it takes this product: beta == 0, EPL
-// elements of B per lane load (FP32: 8 in 32 bytes; BF16 / FP16: 16 in 32
-// bytes; E4M3: 16 in 16 bytes), G = W / EPL lanes per chunk, stores of C and
-// carries 32-byte aligned.  Returns false (nothing launched) otherwise.
-// Measured on the 262k power-law matrix: the group form wins for FP32 storage
-// and 128- or 64-column tiles (N = 128: 84 against 113 us, N = 64: 54 against
-// 61 us); for 32-column FP32 tiles (G = 4) the 32-lane kernel is as fast or
-// faster (41 against 42 us at N = 32).  BF16 / FP16 / E4M3 B: the group form
-// wins from two 128-column tiles on (BF16 N = 256: 155 against 173 us, N =
-// 512: 282 against 335; E4M3 N = 512: 239 against 318), the 32-lane kernel
-// for one (BF16 N = 128: 77 against 84 us; E4M3 equal).
+// elements of B per lane load (FP32: 8 in 32 bytes; BF16 / FP16: 8 in 16
+// bytes; E4M3: 16 in 16 bytes), G = W / EPL lanes per chunk, U rows in
+// flight per worker, stores of C and carries 32-byte aligned.  Returns false
+// (nothing launched) otherwise.  Measured on the 262k power-law matrix: the
+// group form wins for FP32 storage and 128- or 64-column tiles (N = 128: 84
+// against 113 us, N = 64: 54 against 61 us); for 32-column FP32 tiles (G = 4)
+// the 32-lane kernel is as fast or faster (41 against 42 us at N = 32).
+// 2-byte B: 16-lane workers with 16 rows in flight (the registers of 8 FP32
+// rows hold 16 BF16 rows): BF16 N = 128 70.6 against 77.4 us (32-lane), FP16
+// 62.5 against 76.4; N = 512 BF16 254 against 335, FP16 221 against 332.
+// E4M3 B: 8-lane workers, from two 128-column tiles on (N = 512: 239 against
+// 318 us; one tile: equal to the 32-lane kernel).
 template <int W, typename TV, typename TB>
 inline bool launch_grp(const Resolved &r, const KArgs &a, cudaStream_t st)
 {
     constexpr bool f32 = std::is_same<TV, float>::value && std::is_same<TB, float>::value;
-    constexpr int EPL = std::is_same<TB, float>::value ? 8 : 16;
+    constexpr bool b16 = sizeof(TB) == 2;
+    constexpr int EPL = (std::is_same<TB, float>::value || b16) ? 8 : 16;
     constexpr int G = W / EPL;
+    constexpr int U = f32 ? DASPMM_GRP_U : (b16 ? DASPMM_GRP_U16 : DASPMM_GRP_U8);
     constexpr bool grp_ok = f32 ? W >= 64 : W == 128;
     if constexpr (!grp_ok) {
         return false;
@@ -872,13 +879,13 @@ inline bool launch_grp(const Resolved &r, const KArgs &a, cudaStream_t st)
             ((reinterpret_cast<uintptr_t>(a.C) | reinterpret_cast<uintptr_t>(a.slots)) % 32) ==
                 0 &&
             a.ldb % EPL == 0 && a.ldc % 8 == 0 && a.nv % W == 0;
-        if (!(DASPMM_GRP && a.beta == 0.0f && aligned_g && (f32 || r.tiles >= 2))) return false;
+        if (!(DASPMM_GRP && a.beta == 0.0f && aligned_g && (f32 || b16 || r.tiles >= 2)))
+            return false;
         constexpr int NWK = 32 / G;
         const long long groups = ((long long)a.nchunks + NWK - 1) / NWK;
         const unsigned gg = (unsigned)std::max<long long>(
             1, std::min<long long>((groups + 7) / 8, (long long)device_sms() * DASPMM_GRP_MINB));
-        launch_pdl(k_bal_grp<G, EPL, f32 ? DASPMM_GRP_U : DASPMM_GRP_U16, TV, TB>,
-                   dim3(gg, r.tiles), st, a);
+        launch_pdl(k_bal_grp<G, EPL, U, TV, TB>, dim3(gg, r.tiles), st, a);
         return true;
     }
 }
