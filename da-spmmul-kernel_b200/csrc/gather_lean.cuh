@@ -520,7 +520,7 @@ __device__ __forceinline__ void ld_cg_n(float (&r)[VL], const float *p)
     }
 }
 
-// NW 32-bit words (NW = 8: one 32-byte load, 4: one 16-byte load) of B,
+// NW 32-bit words (NW = 8: one 32-byte load, 4: 16 bytes, 2: 8 bytes) of B,
 // read-only path, left packed; elem<TB>() unpacks element i as a float.
 template <int NW>
 __device__ __forceinline__ void ld_raw(uint32_t (&w)[NW], const void *p)
@@ -530,10 +530,13 @@ __device__ __forceinline__ void ld_raw(uint32_t (&w)[NW], const void *p)
         ld8_nc(f, reinterpret_cast<const float *>(p));
 #pragma unroll
         for (int i = 0; i < 8; ++i) w[i] = __float_as_uint(f[i]);
-    } else {
-        static_assert(NW == 4, "16- or 32-byte lane loads");
+    } else if constexpr (NW == 4) {
         const uint4 t = __ldg(reinterpret_cast<const uint4 *>(p));
         w[0] = t.x; w[1] = t.y; w[2] = t.z; w[3] = t.w;
+    } else {
+        static_assert(NW == 2, "8-, 16- or 32-byte lane loads");
+        const uint2 t = __ldg(reinterpret_cast<const uint2 *>(p));
+        w[0] = t.x; w[1] = t.y;
     }
 }
 // acc[0] += a * lo(w), acc[1] += a * hi(w) for two packed 16-bit B elements
@@ -860,33 +863,41 @@ inline void launch_pdl(void (*kernel)(KArgs), dim3 grid, cudaStream_t st, const 
 // 2-byte B: 16-lane workers with 16 rows in flight (the registers of 8 FP32
 // rows hold 16 BF16 rows): BF16 N = 128 70.6 against 77.4 us (32-lane), FP16
 // 62.5 against 76.4; N = 512 BF16 254 against 335, FP16 221 against 332.
-// E4M3 B: 8-lane workers, from two 128-column tiles on (N = 512: 239 against
-// 318 us; one tile: equal to the 32-lane kernel).
+// E4M3 B: for one 128-column tile 16-lane workers with 8-byte loads and 16
+// rows in flight (N = 128: 64.6 against 69.8 us), for more tiles 8-lane
+// workers with 16-byte loads (N = 512: 239 against 318 us; the 16-lane form
+// 247).
+template <int G, int EPL, int U, typename TV, typename TB>
+inline bool launch_grp_as(const Resolved &r, const KArgs &a, cudaStream_t st)
+{
+    const bool aligned_g =
+        (reinterpret_cast<uintptr_t>(a.B) % (EPL * sizeof(TB))) == 0 &&
+        ((reinterpret_cast<uintptr_t>(a.C) | reinterpret_cast<uintptr_t>(a.slots)) % 32) == 0 &&
+        a.ldb % EPL == 0 && a.ldc % 8 == 0 && a.nv % (G * EPL) == 0;
+    if (!(DASPMM_GRP && a.beta == 0.0f && aligned_g)) return false;
+    constexpr int NWK = 32 / G;
+    const long long groups = ((long long)a.nchunks + NWK - 1) / NWK;
+    const unsigned gg = (unsigned)std::max<long long>(
+        1, std::min<long long>((groups + 7) / 8, (long long)device_sms() * DASPMM_GRP_MINB));
+    launch_pdl(k_bal_grp<G, EPL, U, TV, TB>, dim3(gg, r.tiles), st, a);
+    return true;
+}
+
 template <int W, typename TV, typename TB>
 inline bool launch_grp(const Resolved &r, const KArgs &a, cudaStream_t st)
 {
     constexpr bool f32 = std::is_same<TV, float>::value && std::is_same<TB, float>::value;
     constexpr bool b16 = sizeof(TB) == 2;
-    constexpr int EPL = (std::is_same<TB, float>::value || b16) ? 8 : 16;
-    constexpr int G = W / EPL;
-    constexpr int U = f32 ? DASPMM_GRP_U : (b16 ? DASPMM_GRP_U16 : DASPMM_GRP_U8);
-    constexpr bool grp_ok = f32 ? W >= 64 : W == 128;
-    if constexpr (!grp_ok) {
+    if constexpr (f32) {
+        if constexpr (W >= 64) return launch_grp_as<W / 8, 8, DASPMM_GRP_U, TV, TB>(r, a, st);
         return false;
-    } else {
-        const bool aligned_g =
-            (reinterpret_cast<uintptr_t>(a.B) % (EPL * sizeof(TB))) == 0 &&
-            ((reinterpret_cast<uintptr_t>(a.C) | reinterpret_cast<uintptr_t>(a.slots)) % 32) ==
-                0 &&
-            a.ldb % EPL == 0 && a.ldc % 8 == 0 && a.nv % W == 0;
-        if (!(DASPMM_GRP && a.beta == 0.0f && aligned_g && (f32 || b16 || r.tiles >= 2)))
-            return false;
-        constexpr int NWK = 32 / G;
-        const long long groups = ((long long)a.nchunks + NWK - 1) / NWK;
-        const unsigned gg = (unsigned)std::max<long long>(
-            1, std::min<long long>((groups + 7) / 8, (long long)device_sms() * DASPMM_GRP_MINB));
-        launch_pdl(k_bal_grp<G, EPL, U, TV, TB>, dim3(gg, r.tiles), st, a);
-        return true;
+    } else if constexpr (W != 128) {
+        return false;
+    } else if constexpr (b16) {
+        return launch_grp_as<16, 8, DASPMM_GRP_U16, TV, TB>(r, a, st);
+    } else {  // fp8
+        if (r.tiles == 1) return launch_grp_as<16, 8, DASPMM_GRP_U16, TV, TB>(r, a, st);
+        return launch_grp_as<8, 16, DASPMM_GRP_U8, TV, TB>(r, a, st);
     }
 }
 

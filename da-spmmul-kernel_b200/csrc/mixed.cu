@@ -115,12 +115,12 @@ daspmm_status daspmm_spmm_mixed(const daspmm_config *cfg_in, int layout, int nr,
     cfg.alg = DASPMM_ALG_CSR_BALANCED;
     if (cfg.pipe && cfg.pipe != 4) return DASPMM_ERR_UNSUPPORTED;
     cfg.pipe = 4;
-    // measured: 2-byte B (the 16-lane group kernel) runs best, like FP32, at
-    // 96 nonzeros per chunk for one 128-column tile and 128 for wider
-    // products (BF16 N = 128: 71.3 against 74.2 us); E4M3 at 128 for every N.
-    // Never more chunks than the FP32 default, so a workspace sized for it
-    // still suffices.
-    if (!cfg.chunk) cfg.chunk = (nv == 128 && fmt_bytes(b_fmt) == 2) ? 96 : 128;
+    // measured: reduced-precision B (the 16-lane group kernel) runs best, like
+    // FP32, at 96 nonzeros per chunk for one 128-column tile and at 128 for
+    // wider products (BF16 N = 128: 71.3 against 74.2 us; E4M3 64.6 against
+    // 65.4).  Never more chunks than the FP32 default, so a workspace sized
+    // for it still suffices.
+    if (!cfg.chunk) cfg.chunk = nv == 128 ? 96 : 128;
     Resolved r;
     daspmm_status s = resolve(&cfg, layout, nr, nc, nnz, nv, nullptr, C, &r);
     if (s != DASPMM_OK) return s;
