@@ -406,7 +406,8 @@ def run_ours(args):
         if mixed is not None and world == 1:
             mixed["random_1m_deg8"] = run_mixed_random(D, dev, peak)
         batched = None if (args.no_batched or world > 1) else run_batched(D, dev)
-        serving = None if (args.no_serving or world > 1) else run_serving(D, dev, args.serve_seconds)
+        serving = None if (args.no_serving or world > 1) else \
+            run_serving(D, dev, args.serve_seconds, inflight=args.serve_inflight)
         clk = sampler.summary()
         clk_in = sampler.summary(t0, t1)
         clk_sus = sampler.summary(t_s0, t_s1)
@@ -835,7 +836,7 @@ def run_batched(D, dev, reps: int = 20):
             "speedup_vs_plain_graph": round(ms_g / ms_b, 3)}
 
 
-def run_serving(D, dev, seconds: float = 1.0, rate: float = 20000.0):
+def run_serving(D, dev, seconds: float = 1.0, rate: float = 20000.0, inflight: int = 0):
     """The serving configuration: a pool of 64 resident matrices (rows
     log-uniform in [1k, 262k], half uniform-random, half power-law), requests
     with N drawn from {16, 64, 256}, Poisson arrivals (seed 0).  Served with
@@ -863,9 +864,9 @@ def run_serving(D, dev, seconds: float = 1.0, rate: float = 20000.0):
             B32[i, nv] = b
             B16[i, nv] = D.quantize(b, D.Fmt.BF16)
 
-    def stream_of(r, n=None):
-        """n requests at Poisson rate r (seed 0): arrivals, matrix ids, N."""
-        n = n or max(200, int(r * seconds))
+    def stream_of(r, secs):
+        """secs seconds of requests at Poisson rate r (seed 0): arrivals, matrix ids, N."""
+        n = max(200, int(r * secs))
         rng = np.random.default_rng(0)
         return (WL.poisson_arrivals(r, n, seed=0), rng.integers(0, len(pool), n),
                 rng.choice(nvs, n))
@@ -874,10 +875,12 @@ def run_serving(D, dev, seconds: float = 1.0, rate: float = 20000.0):
         A = pool[m]
         return A.nnz * 8 + 4 * (A.nr + 1) + touched[m] * nv * s_b + A.nr * nv * 4
 
-    def run(mode, r, zero=False, max_inflight=0):
+    def run(mode, r, zero=False, max_inflight=None, secs=seconds):
         batched = mode == D.ServeMode.BATCHED
+        if max_inflight is None:
+            max_inflight = inflight if batched else 0
         b_fmt, Bs, s_b = (D.Fmt.BF16, B16, 2) if batched else (D.Fmt.F32, B32, 4)
-        arr, pick, pnv = stream_of(r)
+        arr, pick, pnv = stream_of(r, secs)
         if zero:
             arr = np.zeros(arr.size)
         srv = D.Server(budget_bytes=8 << 30, mode=mode, b_fmt=b_fmt, max_inflight=max_inflight)
@@ -903,6 +906,7 @@ def run_serving(D, dev, seconds: float = 1.0, rate: float = 20000.0):
     B_, P_ = D.ServeMode.BATCHED, D.ServeMode.PLAIN
     n = int(rate * seconds)
     out = {"pool": len(pool), "requests": n, "offered_req_s": rate, "nv": list(nvs),
+           "batched_max_inflight": inflight or "library default (2)",
            "pool_nnz": int(sum(A.nnz for A in pool)),
            "batched_bf16": run(B_, rate), "plain_fp32": run(P_, rate)}
     cap_b = run(B_, rate, zero=True)
@@ -916,19 +920,20 @@ def run_serving(D, dev, seconds: float = 1.0, rate: float = 20000.0):
     # fraction f of its capacity (so the plain throughput at that bound is f x
     # its capacity); the batched mode's throughput at the bound is its highest
     # offered Poisson rate that keeps up (>= 97 %) within that p99, found by
-    # bisection between f x the plain capacity and 2 x its own capacity.
+    # bisection between f x the plain capacity and 2 x its own capacity.  Each
+    # point runs 2 s of requests (p99 over >= 20,000 latencies).
     keeps_up = lambda q, r, b: q["p99_us"] <= b and q["req_s"] >= 0.97 * r
     eq = []
     for f in (0.5, 0.75, 0.9):
         rp_ = f * cap_p["req_s"]
-        plain_f = run(P_, rp_)
+        plain_f = run(P_, rp_, secs=2.0)
         bound = plain_f["p99_us"]
         lo, hi = rp_, 2.0 * cap_b["req_s"]
-        best = run(B_, lo)
+        best = run(B_, lo, secs=2.0)
         if keeps_up(best, lo, bound):
             for _ in range(5):
                 mid = 0.5 * (lo + hi)
-                q = run(B_, mid)
+                q = run(B_, mid, secs=2.0)
                 if keeps_up(q, mid, bound):
                     lo, best = mid, q
                 else:
@@ -941,7 +946,7 @@ def run_serving(D, dev, seconds: float = 1.0, rate: float = 20000.0):
                         "rule": "bound = plain FP32 p99 at the given fraction of its capacity; "
                                 "batched: the highest offered Poisson rate (bisection) whose "
                                 "p99 stays within the bound and whose throughput keeps up "
-                                "(>= 97%)"}
+                                "(>= 97%); 2 s of requests per point"}
     out["sweep"] = {"batched_bf16": [run(B_, r) for r in (10e3, 20e3, 40e3, 60e3, 80e3)],
                     "plain_fp32": [run(P_, r) for r in (5e3, 10e3, 15e3, 20e3)]}
     hot = 0.9 * cap_b["req_s"]
@@ -1033,6 +1038,8 @@ def main():
     ap.add_argument("--no-variants", action="store_true",
                     help="skip the per-variant timing of this library's design space")
     ap.add_argument("--serve-seconds", type=float, default=1.0)
+    ap.add_argument("--serve-inflight", type=int, default=0,
+                    help="launch groups in flight for the batched server (0 = library default)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
