@@ -328,10 +328,14 @@ __device__ __forceinline__ void batch_item(const BatchInst &I, const BatchTile &
         batch_rows<W, DASPMM_LEAN_U, TV, TB>(I, T.row0, T.row1, ct * W, pol_once);
 }
 
+#ifndef DASPMM_BATCH_MINB
+#define DASPMM_BATCH_MINB DASPMM_LEAN_MINB  // CTAs of 256 threads per SM
+#endif
+
 // WM: the tile width every instance uses, or 0 for a batch of mixed widths
 // (a warp-uniform switch on the item's instance).
 template <int WM, typename TV, typename TB>
-__global__ void __launch_bounds__(256, DASPMM_LEAN_MINB)
+__global__ void __launch_bounds__(256, DASPMM_BATCH_MINB)
     k_batch_spmm(const BatchInst *__restrict__ inst, const BatchItem *__restrict__ items,
                  long long nitems, unsigned long long *head)
 {
@@ -362,7 +366,7 @@ void launch_batch_w(const BatchInst *d_inst, const BatchItem *d_items, long long
                     unsigned long long *d_head, cudaStream_t st)
 {
     const unsigned grid = (unsigned)std::max<long long>(
-        1, std::min<long long>((long long)device_sms() * DASPMM_LEAN_MINB, (nitems + 7) / 8));
+        1, std::min<long long>((long long)device_sms() * DASPMM_BATCH_MINB, (nitems + 7) / 8));
     k_batch_spmm<WM, TV, TB><<<grid, 256, 0, st>>>(d_inst, d_items, nitems, d_head);
 }
 

@@ -630,6 +630,10 @@ static __device__ __noinline__ void piece_arrive_grp(const int *__restrict__ row
 #ifndef DASPMM_GRP_MINB
 #define DASPMM_GRP_MINB 2   // CTAs of 256 threads per SM: 16 warps, <= 128 registers
 #endif
+// 16-byte FP32 lane loads (32-column tiles) hold half the registers per row in
+// flight: 3 CTAs per SM (24 warps, <= 85 registers)
+#define DASPMM_GRP_MINB_OF(EPL, TB) \
+    ((EPL) == 4 && std::is_same<TB, float>::value ? 3 : DASPMM_GRP_MINB)
 
 // k_bal_fast with G-lane workers, beta == 0.  Each worker (G consecutive
 // lanes) takes one chunk of a group (32/G consecutive chunks per warp) and
@@ -650,7 +654,7 @@ static __device__ __noinline__ void piece_arrive_grp(const int *__restrict__ row
 // one after the other.  B aligned to EPL*sizeof(TB) bytes, C and the carry
 // slots to 32 bytes.
 template <int G, int EPL, int U, typename TV = float, typename TB = float>
-__global__ void __launch_bounds__(256, DASPMM_GRP_MINB) k_bal_grp(const KArgs a)
+__global__ void __launch_bounds__(256, DASPMM_GRP_MINB_OF(EPL, TB)) k_bal_grp(const KArgs a)
 {
     constexpr int NW = 32 / G;                             // workers per warp
     constexpr int RAW = EPL * (int)sizeof(TB) / 4;         // 32-bit words per lane load
@@ -858,8 +862,9 @@ inline void launch_pdl(void (*kernel)(KArgs), dim3 grid, cudaStream_t st, const 
 // flight per worker, stores of C and carries 32-byte aligned.  Returns false
 // (nothing launched) otherwise.  Measured on the 262k power-law matrix: the
 // group form wins for FP32 storage and 128- or 64-column tiles (N = 128: 84
-// against 113 us, N = 64: 54 against 61 us); for 32-column FP32 tiles (G = 4)
-// the 32-lane kernel is as fast or faster (41 against 42 us at N = 32).
+// against 113 us, N = 64: 54 against 61 us); 32-column FP32 tiles take 8-lane
+// workers with 16-byte loads at 24 warps per SM (N = 32: 36 against 41 us
+// for the 32-lane kernel; 4-lane workers with 32-byte loads 42 us).
 // 2-byte B: 16-lane workers with 16 rows in flight (the registers of 8 FP32
 // rows hold 16 BF16 rows): BF16 N = 128 70.6 against 77.4 us (32-lane), FP16
 // 62.5 against 76.4; N = 512 BF16 254 against 335, FP16 221 against 332.
@@ -878,7 +883,8 @@ inline bool launch_grp_as(const Resolved &r, const KArgs &a, cudaStream_t st)
     constexpr int NWK = 32 / G;
     const long long groups = ((long long)a.nchunks + NWK - 1) / NWK;
     const unsigned gg = (unsigned)std::max<long long>(
-        1, std::min<long long>((groups + 7) / 8, (long long)device_sms() * DASPMM_GRP_MINB));
+        1, std::min<long long>((groups + 7) / 8,
+                               (long long)device_sms() * DASPMM_GRP_MINB_OF(EPL, TB)));
     launch_pdl(k_bal_grp<G, EPL, U, TV, TB>, dim3(gg, r.tiles), st, a);
     return true;
 }
@@ -890,7 +896,7 @@ inline bool launch_grp(const Resolved &r, const KArgs &a, cudaStream_t st)
     constexpr bool b16 = sizeof(TB) == 2;
     if constexpr (f32) {
         if constexpr (W >= 64) return launch_grp_as<W / 8, 8, DASPMM_GRP_U, TV, TB>(r, a, st);
-        return false;
+        else return launch_grp_as<8, 4, DASPMM_GRP_U, TV, TB>(r, a, st);
     } else if constexpr (W != 128) {
         return false;
     } else if constexpr (b16) {
