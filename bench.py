@@ -904,11 +904,18 @@ def run_serving(D, dev, seconds: float = 1.0, rate: float = 20000.0, inflight: i
                 "max_group": int(st["max_group"])}
 
     B_, P_ = D.ServeMode.BATCHED, D.ServeMode.PLAIN
+
+    def median_run(mode, r, secs=seconds):
+        """The run with the median p99 of three (a host-side stall of a few
+        ms in one run sets that run's p99), with all three p99s."""
+        runs = sorted((run(mode, r, secs=secs) for _ in range(3)), key=lambda q: q["p99_us"])
+        return dict(runs[1], p99_us_runs=[q["p99_us"] for q in runs])
+
     n = int(rate * seconds)
     out = {"pool": len(pool), "requests": n, "offered_req_s": rate, "nv": list(nvs),
            "batched_max_inflight": inflight or "library default (2)",
            "pool_nnz": int(sum(A.nnz for A in pool)),
-           "batched_bf16": run(B_, rate), "plain_fp32": run(P_, rate)}
+           "batched_bf16": median_run(B_, rate), "plain_fp32": median_run(P_, rate)}
     cap_b = run(B_, rate, zero=True)
     cap_p = run(P_, rate, zero=True)
     out["capacity"] = {"batched_bf16_req_s": cap_b["req_s"], "plain_fp32_req_s": cap_p["req_s"],
@@ -921,12 +928,14 @@ def run_serving(D, dev, seconds: float = 1.0, rate: float = 20000.0, inflight: i
     # its capacity); the batched mode's throughput at the bound is its highest
     # offered Poisson rate that keeps up (>= 97 %) within that p99, found by
     # bisection between f x the plain capacity and 2 x its own capacity.  Each
-    # point runs 2 s of requests (p99 over >= 20,000 latencies).
+    # point runs 2 s of requests (p99 over >= 20,000 latencies).  The plain
+    # path near saturation is noisy (a run that falls behind has a p99 of
+    # seconds), so its bound is the median p99 of three runs.
     keeps_up = lambda q, r, b: q["p99_us"] <= b and q["req_s"] >= 0.97 * r
     eq = []
     for f in (0.5, 0.75, 0.9):
         rp_ = f * cap_p["req_s"]
-        plain_f = run(P_, rp_, secs=2.0)
+        plain_f = median_run(P_, rp_, secs=2.0)
         bound = plain_f["p99_us"]
         lo, hi = rp_, 2.0 * cap_b["req_s"]
         best = run(B_, lo, secs=2.0)
@@ -939,11 +948,14 @@ def run_serving(D, dev, seconds: float = 1.0, rate: float = 20000.0, inflight: i
                 else:
                     hi = mid
         eq.append({"plain_load_fraction": f, "p99_bound_us": bound,
+                   "plain_p99_us_runs": plain_f["p99_us_runs"],
+                   "plain_kept_up": plain_f["req_s"] >= 0.97 * rp_,
                    "plain_req_s": plain_f["req_s"], "batched_req_s": best["req_s"],
                    "batched_p99_us": best["p99_us"],
                    "ratio": round(best["req_s"] / max(plain_f["req_s"], 1e-9), 3)})
     out["equal_p99"] = {"points": eq,
-                        "rule": "bound = plain FP32 p99 at the given fraction of its capacity; "
+                        "rule": "bound = plain FP32 p99 at the given fraction of its capacity "
+                                "(median of 3 runs); "
                                 "batched: the highest offered Poisson rate (bisection) whose "
                                 "p99 stays within the bound and whose throughput keeps up "
                                 "(>= 97%); 2 s of requests per point"}
