@@ -383,10 +383,10 @@ def run_ours(args):
         # CPU baseline: the reference's host loop, 1 thread (it is serial), full matrix
         cpu = None
         if world == 1 and not args.no_cpu:
-            ms_cpu, nnz_s, _, kind, cores = cpu_reference_time(A, B, NV, 1, 3)
+            ms_cpu, nnz_s, _, kind, cores = cpu_reference_time(A, B, NV, 1, 5)
             cpu = {"value": round(2.0 * nnz_s * NV / (ms_cpu * 1e-3) / 1e9, 3), "unit": UNIT,
-                   "cores": cores, "kind": kind,
-                   "sample": f"full matrix ({nnz_s} nnz, N=128), median of 3 passes, 1 thread"}
+                   "cores": cores, "kind": kind, "host_cores": os.cpu_count(),
+                   "sample": f"full matrix ({nnz_s} nnz, N=128), median of 5 passes, 1 thread"}
         # NVTX ranges name the sections for a profiler's kernel filter
         # (ncu --nvtx --nvtx-include "variants/")
         nvtx = torch.cuda.nvtx
