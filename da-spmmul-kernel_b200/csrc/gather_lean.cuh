@@ -533,10 +533,12 @@ __device__ __forceinline__ void ld_raw(uint32_t (&w)[NW], const void *p)
     } else if constexpr (NW == 4) {
         const uint4 t = __ldg(reinterpret_cast<const uint4 *>(p));
         w[0] = t.x; w[1] = t.y; w[2] = t.z; w[3] = t.w;
-    } else {
-        static_assert(NW == 2, "8-, 16- or 32-byte lane loads");
+    } else if constexpr (NW == 2) {
         const uint2 t = __ldg(reinterpret_cast<const uint2 *>(p));
         w[0] = t.x; w[1] = t.y;
+    } else {
+        static_assert(NW == 1, "4-, 8-, 16- or 32-byte lane loads");
+        w[0] = __ldg(reinterpret_cast<const unsigned int *>(p));
     }
 }
 // acc[0] += a * lo(w), acc[1] += a * hi(w) for two packed 16-bit B elements
@@ -630,10 +632,6 @@ static __device__ __noinline__ void piece_arrive_grp(const int *__restrict__ row
 #ifndef DASPMM_GRP_MINB
 #define DASPMM_GRP_MINB 2   // CTAs of 256 threads per SM: 16 warps, <= 128 registers
 #endif
-// 16-byte FP32 lane loads (32-column tiles) hold half the registers per row in
-// flight: 3 CTAs per SM (24 warps, <= 85 registers)
-#define DASPMM_GRP_MINB_OF(EPL, TB) \
-    ((EPL) == 4 && std::is_same<TB, float>::value ? 3 : DASPMM_GRP_MINB)
 
 // k_bal_fast with G-lane workers, beta == 0.  Each worker (G consecutive
 // lanes) takes one chunk of a group (32/G consecutive chunks per warp) and
@@ -653,8 +651,9 @@ static __device__ __noinline__ void piece_arrive_grp(const int *__restrict__ row
 // dispatched first, so with several tiles their B column slabs are gathered
 // one after the other.  B aligned to EPL*sizeof(TB) bytes, C and the carry
 // slots to 32 bytes.
-template <int G, int EPL, int U, typename TV = float, typename TB = float>
-__global__ void __launch_bounds__(256, DASPMM_GRP_MINB_OF(EPL, TB)) k_bal_grp(const KArgs a)
+template <int G, int EPL, int U, typename TV = float, typename TB = float,
+          int MINB = DASPMM_GRP_MINB, bool WS = false>
+__global__ void __launch_bounds__(256, MINB) k_bal_grp(const KArgs a)
 {
     constexpr int NW = 32 / G;                             // workers per warp
     constexpr int RAW = EPL * (int)sizeof(TB) / 4;         // 32-bit words per lane load
@@ -711,17 +710,38 @@ __global__ void __launch_bounds__(256, DASPMM_GRP_MINB_OF(EPL, TB)) k_bal_grp(co
             int prev = __shfl_up_sync(kFull, E, 1, G);
             if (gl == 0) prev = rstart;
             empty_row = (__ballot_sync(kFull, have && r + gl < s1 && E == prev) & gmask) != 0;
-            int last = __shfl_sync(kFull, E, G - 1, G);
             bool more = have && !empty_row && r + G < s1;
-            for (int rb = r + G; __any_sync(kFull, more); rb += G) {
-                int e2 = 0;
-                if (more) e2 = __ldg(a.rowPtr + min(rb + 1 + gl, a.nr));
-                int p2 = __shfl_up_sync(kFull, e2, 1, G);
-                if (gl == 0) p2 = last;
-                const unsigned b2 = __ballot_sync(kFull, more && rb + gl < s1 && e2 == p2);
-                if (more) empty_row = (b2 & gmask) != 0;
-                last = __shfl_sync(kFull, e2, G - 1, G);
-                more = more && !empty_row && rb + G < s1;
+            if constexpr (WS) {
+                // the rest of the chunk's rows, 32 per step: lane gl of a worker
+                // checks rows rb + gl*K .. rb + gl*K + K - 1 (K + 1 independent
+                // loads) -- one load latency per 32 rows instead of per G
+                constexpr int K = 32 / G;
+                for (int rb = r + G; __any_sync(kFull, more); rb += 32) {
+                    bool e = false;
+                    if (more) {
+                        const int k0 = rb + gl * K;
+                        int q[K + 1];
+#pragma unroll
+                        for (int j = 0; j <= K; ++j) q[j] = __ldg(a.rowPtr + min(k0 + j, a.nr));
+#pragma unroll
+                        for (int j = 0; j < K; ++j) e |= k0 + j < s1 && q[j + 1] == q[j];
+                    }
+                    const unsigned b2 = __ballot_sync(kFull, e);
+                    if (more) empty_row = (b2 & gmask) != 0;
+                    more = more && !empty_row && rb + 32 < s1;
+                }
+            } else {
+                int last = __shfl_sync(kFull, E, G - 1, G);
+                for (int rb = r + G; __any_sync(kFull, more); rb += G) {
+                    int e2 = 0;
+                    if (more) e2 = __ldg(a.rowPtr + min(rb + 1 + gl, a.nr));
+                    int p2 = __shfl_up_sync(kFull, e2, 1, G);
+                    if (gl == 0) p2 = last;
+                    const unsigned b2 = __ballot_sync(kFull, more && rb + gl < s1 && e2 == p2);
+                    if (more) empty_row = (b2 & gmask) != 0;
+                    last = __shfl_sync(kFull, e2, G - 1, G);
+                    more = more && !empty_row && rb + G < s1;
+                }
             }
         }
         const bool skip = !have || empty_row || !pad_ok;
@@ -863,8 +883,9 @@ inline void launch_pdl(void (*kernel)(KArgs), dim3 grid, cudaStream_t st, const 
 // (nothing launched) otherwise.  Measured on the 262k power-law matrix: the
 // group form wins for FP32 storage and 128- or 64-column tiles (N = 128: 84
 // against 113 us, N = 64: 54 against 61 us); 32-column FP32 tiles take 8-lane
-// workers with 16-byte loads at 24 warps per SM (N = 32: 36 against 41 us
-// for the 32-lane kernel; 4-lane workers with 32-byte loads 42 us).
+// workers with 16-byte loads at 24 warps per SM and the chunk scan 32 rows per
+// step (N = 32: 34.3 against 41 us for the 32-lane kernel; 4-lane workers with
+// 32-byte loads 42 us; on the 1M uniform-random matrix 187 against 293 us).
 // 2-byte B: 16-lane workers with 16 rows in flight (the registers of 8 FP32
 // rows hold 16 BF16 rows): BF16 N = 128 70.6 against 77.4 us (32-lane), FP16
 // 62.5 against 76.4; N = 512 BF16 254 against 335, FP16 221 against 332.
@@ -872,7 +893,8 @@ inline void launch_pdl(void (*kernel)(KArgs), dim3 grid, cudaStream_t st, const 
 // rows in flight (N = 128: 64.6 against 69.8 us), for more tiles 8-lane
 // workers with 16-byte loads (N = 512: 239 against 318 us; the 16-lane form
 // 247).
-template <int G, int EPL, int U, typename TV, typename TB>
+template <int G, int EPL, int U, typename TV, typename TB, int MINB = DASPMM_GRP_MINB,
+          bool WS = false>
 inline bool launch_grp_as(const Resolved &r, const KArgs &a, cudaStream_t st)
 {
     const bool aligned_g =
@@ -884,9 +906,26 @@ inline bool launch_grp_as(const Resolved &r, const KArgs &a, cudaStream_t st)
     const long long groups = ((long long)a.nchunks + NWK - 1) / NWK;
     const unsigned gg = (unsigned)std::max<long long>(
         1, std::min<long long>((groups + 7) / 8,
-                               (long long)device_sms() * DASPMM_GRP_MINB_OF(EPL, TB)));
-    launch_pdl(k_bal_grp<G, EPL, U, TV, TB>, dim3(gg, r.tiles), st, a);
+                               (long long)device_sms() * MINB));
+    launch_pdl(k_bal_grp<G, EPL, U, TV, TB, MINB, WS>, dim3(gg, r.tiles), st, a);
     return true;
+}
+
+// Reduced-precision B in 32- and 64-column tiles: workers of W / E lanes with
+// 8-byte lane loads of E elements (BF16 / FP16: 4, E4M3: 8), 3 CTAs per SM
+// (24 warps, <= 85 registers).  Measured on the 262k power-law and the 1M
+// uniform-random matrix against the 32-lane kernel (us): N = 32 BF16 35.1 /
+// 152 against 47.0 / 278, FP16 34.8 / 150 against 47.1 / 278, E4M3 44.9 / 130
+// against 48.4 / 228; N = 64 BF16 44.9 / 229 against 64.9 / 515, FP16 42.9 /
+// 225 against 48.4 / 352, E4M3 45.6 / 197 against 49.9 / 304.  16-byte loads,
+// 4-byte loads, and 2 or 4 CTAs per SM measured slower overall.  The chunk
+// scan 32 rows per step pays except for FP16 (fma.rn.f32.f16) 32-column tiles.
+template <int W, typename TV, typename TB>
+inline bool launch_grp_narrow(const Resolved &r, const KArgs &a, cudaStream_t st)
+{
+    constexpr int E = sizeof(TB) == 2 ? 4 : 8;
+    constexpr bool ws = !(W == 32 && std::is_same<TV, fp16>::value && std::is_same<TB, fp16>::value);
+    return launch_grp_as<W / E, E, 16, TV, TB, 3, ws>(r, a, st);
 }
 
 template <int W, typename TV, typename TB>
@@ -896,9 +935,9 @@ inline bool launch_grp(const Resolved &r, const KArgs &a, cudaStream_t st)
     constexpr bool b16 = sizeof(TB) == 2;
     if constexpr (f32) {
         if constexpr (W >= 64) return launch_grp_as<W / 8, 8, DASPMM_GRP_U, TV, TB>(r, a, st);
-        else return launch_grp_as<8, 4, DASPMM_GRP_U, TV, TB>(r, a, st);
+        else return launch_grp_as<8, 4, DASPMM_GRP_U, TV, TB, 3, true>(r, a, st);  // 24 warps
     } else if constexpr (W != 128) {
-        return false;
+        return launch_grp_narrow<W, TV, TB>(r, a, st);
     } else if constexpr (b16) {
         return launch_grp_as<16, 8, DASPMM_GRP_U16, TV, TB>(r, a, st);
     } else {  // fp8

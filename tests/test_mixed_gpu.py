@@ -219,14 +219,15 @@ def test_config3_full_size_error_bound(cuda):
 
 
 def test_group_kernel_equals_32_lane_kernel_mixed(mats):
-    """Reduced-precision B with two or more 128-column tiles runs the worker-
-    group window kernel when C is 32-byte aligned, the 32-lane one when C is
-    16 bytes off: same chunks and order of summation, bit-identical C."""
+    """Reduced-precision B runs the worker-group window kernel (8-byte lane
+    loads for 32- and 64-column tiles, 16-byte ones for 128) when C is
+    32-byte aligned, the 32-lane one when C is 16 bytes off: same chunks and
+    order of summation, bit-identical C.  The hub matrix has empty rows."""
     import torch
     rng = np.random.default_rng(31)
-    for name in ("powerlaw", "random"):
+    for name in ("powerlaw", "random", "hub"):
         A, dA = mats[name]
-        for nv in (128, 256, 384):
+        for nv in (32, 64, 128, 256, 384):
             B = rng.uniform(-1, 1, A.nc * nv).astype(np.float32)
             for vf, bf in ((D.Fmt.BF16, D.Fmt.BF16), (D.Fmt.F16, D.Fmt.F16),
                            (D.Fmt.BF16, D.Fmt.E4M3), (D.Fmt.F32, D.Fmt.E4M3)):

@@ -346,15 +346,32 @@ def test_full_size_configs(cuda):
         _check(A2, 0, nv, B, C, what=f"cfg2 {alg.name}")
 
 
+def _sparse_empty_rows(nr, nc, seed):
+    """Rows of 1-3 nonzeros with about 1 % empty rows and a few hub rows: a
+    chunk's empty row often lies far beyond its first rows, so the window
+    kernels' scan for it runs several steps."""
+    rng = np.random.default_rng(seed)
+    lens = rng.integers(1, 4, nr)
+    lens[rng.random(nr) < 0.01] = 0
+    lens[rng.integers(0, nr, 4)] = 700
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    ci = np.concatenate([np.sort(rng.choice(nc, int(k), replace=False)) for k in lens]
+                        ).astype(np.int32)
+    va = rng.uniform(-1, 1, int(rp[-1])).astype(np.float32)
+    return D.Csr(nr, nc, rp, ci, va)
+
+
 def test_group_kernel_equals_32_lane_kernel(cuda):
     """FP32 row-major balanced CSR: with B and C 32-byte aligned the worker-
-    group window kernel runs (G = 16 / 8 / 4 lanes per chunk for 128 / 64 /
+    group window kernel runs (G = 16 / 8 / 8 lanes per chunk for 128 / 64 /
     32-column tiles), with both 16 bytes off that alignment the 32-lane one.
     Same chunks and order of summation: the products are bit-identical,
-    whatever the tile width."""
+    whatever the tile width.  The third matrix puts empty rows deep inside
+    chunks: both kernels must hand exactly those chunks to the walk kernel."""
     import torch
     rng = np.random.default_rng(12)
-    for A in (D.gen_powerlaw(20000, dmax=2000, seed=8), D.gen_random(5000, 4000, 5.0, seed=9)):
+    for A in (D.gen_powerlaw(20000, dmax=2000, seed=8), D.gen_random(5000, 4000, 5.0, seed=9),
+              _sparse_empty_rows(6000, 5000, 13)):
         dA = D.DeviceCsr(A)
         for nv in (32, 64, 96, 128, 256):
             B = rng.uniform(-1, 1, A.nc * nv).astype(np.float32)
