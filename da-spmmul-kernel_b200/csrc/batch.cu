@@ -331,6 +331,9 @@ __device__ __forceinline__ void batch_item(const BatchInst &I, const BatchTile &
 #ifndef DASPMM_BATCH_MINB
 #define DASPMM_BATCH_MINB DASPMM_LEAN_MINB  // CTAs of 256 threads per SM
 #endif
+#ifndef DASPMM_BATCH_GRP
+#define DASPMM_BATCH_GRP 1  // runs of rows take the worker-group gather
+#endif
 
 // WM: the tile width every instance uses, or 0 for a batch of mixed widths
 // (a warp-uniform switch on the item's instance).
@@ -359,6 +362,225 @@ __global__ void __launch_bounds__(256, DASPMM_BATCH_MINB)
     }
 }
 
+// One item of instance *I, column tile ct, for the G lanes of this worker
+// (one of the warp's 32 / G workers, each on its own item, all in step),
+// gathered like the single-product group kernel: windows of G nonzeros, one
+// lane load of EPL elements per lane and row, UU rows in flight.  A run of
+// whole rows without empty rows (beta == 0) stores each row at its bit of the
+// window's row-end mask; a piece of a long row sums its nonzeros, leaves the
+// partial in its slot and, if it is the row's last piece to arrive, adds the
+// slots in piece order and stores the row.  The same FMAs and additions in
+// the same order as batch_rows_fast and batch_piece, so an item gives the
+// same bits on either path.  Positions past the worker's last nonzero load
+// nothing and add an exact zero.
+template <int G, int EPL, int U, typename TV, typename TB>
+__device__ __forceinline__ void batch_item_grp(const BatchInst *__restrict__ I,
+                                               const BatchTile &T, int ct, bool have,
+                                               uint64_t pol_once)
+{
+    constexpr int RAW = EPL * (int)sizeof(TB) / 4;  // 32-bit words per lane load
+    constexpr int UU = U < G ? U : G;
+    constexpr unsigned GM = G == 32 ? 0xFFFFFFFFu : ((1u << G) - 1u);
+    constexpr bool SCALED = std::is_same<TB, fp8>::value;
+    const int lane = threadIdx.x & 31, w = lane / G, gl = lane % G;
+    const unsigned gmask = GM << (G * w);
+    const int col = ct * (G * EPL) + gl * EPL;
+    const bool piece = have && T.piece >= 0;
+    const int *rp = have ? I->rowPtr : nullptr;
+    const int *ci = have ? I->colIdx : nullptr;
+    const TV *Av = have ? reinterpret_cast<const TV *>(I->vals) : nullptr;
+    const TB *Bl = have ? reinterpret_cast<const TB *>(I->B) + col : nullptr;
+    const int ldb = have ? I->ldb : 0, ldc = have ? I->ldc : 0, nr = have ? I->nr : 0;
+    const int row1 = have ? T.row1 : 0;
+    const int k0 = !have ? 0 : (piece ? T.k0 : __ldg(rp + T.row0));
+    const int k1 = !have ? 0 : (piece ? T.k1 : __ldg(rp + T.row1));
+    int r = have ? T.row0 : 0;
+    int E = (have && !piece) ? __ldg(rp + min(r + 1 + gl, nr)) : 0;
+    int nwin = (k1 - k0 + G - 1) / G;
+#pragma unroll
+    for (int o = G; o < 32; o <<= 1) nwin = max(nwin, __shfl_xor_sync(kFull, nwin, o));
+    float acc[EPL];
+#pragma unroll
+    for (int e = 0; e < EPL; ++e) acc[e] = 0.0f;
+    auto load_win = [&](int wb, int &c, float &v) {
+        const bool ok = wb + gl < k1;
+        c = ok ? ld_hint_s32(ci + wb + gl, pol_once) : 0;
+        v = ok ? ld_val<TV>(Av + wb + gl, pol_once) : 0.0f;
+    };
+    int ccur, cnext;
+    float vcur, vnext;
+    int wb = k0;
+    load_win(wb, ccur, vcur);
+    for (int wi = 0; wi < nwin; ++wi, wb += G) {
+        load_win(wb + G, cnext, vnext);
+        const int cnt = k1 - wb;  // nonzeros of this worker left (<= 0: none)
+        const int pos = E - 1 - wb;
+        const bool in = have && !piece && r + gl < row1 && pos >= 0 && pos < min(cnt, G);
+        const unsigned e32 = __reduce_or_sync(kFull, in ? (1u << (pos + G * w)) : 0u);
+        const unsigned ends = (e32 >> (G * w)) & GM;
+        if (have && !piece) E = __ldg(rp + min(r + __popc(ends) + 1 + gl, nr));  // next window's
+        float *cdst = (have && !piece) ? I->C + (size_t)r * ldc + col : nullptr;
+#pragma unroll
+        for (int g = 0; g < G / UU; ++g) {
+            int cc[UU];
+            float vv[UU];
+#pragma unroll
+            for (int u = 0; u < UU; ++u) {
+                cc[u] = __shfl_sync(kFull, ccur, g * UU + u, G);
+                vv[u] = __shfl_sync(kFull, vcur, g * UU + u, G);
+            }
+            uint32_t b[UU][RAW];
+#pragma unroll
+            for (int u = 0; u < UU; ++u) {
+                if (g * UU + u < cnt) {
+                    ld_raw<RAW>(b[u], Bl + (size_t)cc[u] * ldb);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < RAW; ++i) b[u][i] = 0u;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < UU; ++u) {
+#pragma unroll
+                for (int e = 0; e < EPL; ++e)
+                    acc[e] = fmaf(vv[u], elem<TB, RAW>(b[u], e), acc[e]);
+                if ((ends >> (g * UU + u)) & 1u) {
+                    if constexpr (SCALED) {
+#pragma unroll
+                        for (int e = 0; e < EPL; ++e) acc[e] *= __ldg(I->bscale + col + e);
+                    }
+                    st_hint_n<EPL>(cdst, acc, pol_once);
+#pragma unroll
+                    for (int e = 0; e < EPL; ++e) acc[e] = 0.0f;
+                    ++r;
+                    cdst += ldc;
+                }
+            }
+            asm volatile("" ::: "memory");
+        }
+        ccur = cnext;
+        vcur = vnext;
+    }
+    if (!piece) return;
+    // the piece's partial, then the row's last piece adds all of them
+    const int nv = I->nv;
+    float *slot0 = I->slots + (size_t)T.slot * nv + col;
+    st_n<EPL>(slot0 + (size_t)T.piece * nv, acc);
+    __threadfence();
+    __syncwarp(gmask);
+    int *counter = I->cnt + (size_t)T.cnt * I->col_tiles + ct;
+    int last = 0;
+    if (gl == 0) last = atomicAdd(counter, 1) == T.npieces - 1;
+    last = __shfl_sync(gmask, last, 0, G);
+    if (!last) return;
+    __threadfence();
+    if (gl == 0) *counter = 0;  // every piece has arrived: ready for the next run
+    float tot[EPL];
+#pragma unroll
+    for (int e = 0; e < EPL; ++e) tot[e] = 0.0f;
+    for (int p = 0; p < T.npieces; ++p) {
+        float h[EPL];
+        if (p == T.piece) {
+#pragma unroll
+            for (int e = 0; e < EPL; ++e) h[e] = acc[e];
+        } else {
+            ld_cg_n<EPL>(h, slot0 + (size_t)p * nv);
+        }
+#pragma unroll
+        for (int e = 0; e < EPL; ++e) tot[e] += h[e];
+    }
+    if constexpr (SCALED) {
+#pragma unroll
+        for (int e = 0; e < EPL; ++e) tot[e] *= __ldg(I->bscale + col + e);
+    }
+    st_n<EPL>(I->C + (size_t)T.row0 * ldc + col, tot);
+}
+
+// The persistent batch kernel with G-lane workers: a warp claims 32 / G
+// consecutive items; the runs without empty rows and the pieces of long rows
+// (beta == 0, tile width WG, 32-byte aligned B, C and slots) are gathered
+// together by batch_item_grp, every other item (runs with empty rows, other
+// widths) by the whole warp with batch_item after it.
+template <int WG, int G, int EPL, int U, typename TV, typename TB, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+    k_batch_grp(const BatchInst *__restrict__ inst, const BatchItem *__restrict__ items,
+                long long nitems, unsigned long long *head)
+{
+    static_assert(G * EPL == WG, "a worker covers one column tile");
+    constexpr int NW = 32 / G;
+    const uint64_t pol_once = policy_evict_first();
+    const int lane = threadIdx.x & 31, w = lane / G;
+    for (;;) {
+        unsigned long long g0 = 0;
+        if (lane == 0) g0 = atomicAdd(head, (unsigned long long)NW);
+        g0 = __shfl_sync(kFull, g0, 0);
+        if (g0 >= (unsigned long long)nitems) return;
+        const long long gi = (long long)g0 + w;
+        const bool valid = gi < nitems;
+        BatchItem it{};
+        const BatchInst *I = nullptr;
+        BatchTile T{};
+        if (valid) {
+            it = items[gi];
+            I = inst + it.inst;
+            T = I->tiles[it.tile];
+        }
+        const bool fast = valid && I->grp && I->W == WG && I->beta == 0.0f &&
+                          (T.piece >= 0 ? (reinterpret_cast<uintptr_t>(I->slots) & 31) == 0
+                                        : T.npieces == 0);
+        if (__any_sync(kFull, fast))
+            batch_item_grp<G, EPL, U, TV, TB>(I, T, it.ctile, fast, pol_once);
+        unsigned slow = __ballot_sync(kFull, valid && !fast && lane % G == 0);
+        while (slow) {  // warp-uniform
+            const int l = __ffs(slow) - 1;
+            slow &= slow - 1;
+            const BatchItem it2 = items[(long long)g0 + l / G];
+            const BatchInst &I2 = inst[it2.inst];
+            const BatchTile T2 = I2.tiles[it2.tile];
+            if (I2.W == 128) batch_item<128, TV, TB>(I2, T2, it2.ctile, pol_once);
+            else if (I2.W == 64) batch_item<64, TV, TB>(I2, T2, it2.ctile, pol_once);
+            else batch_item<32, TV, TB>(I2, T2, it2.ctile, pol_once);
+        }
+    }
+}
+
+template <int WG, int G, int EPL, int U, typename TV, typename TB, int MINB>
+void launch_batch_grp(const BatchInst *d_inst, const BatchItem *d_items, long long nitems,
+                      unsigned long long *d_head, cudaStream_t st)
+{
+    const long long claims = (nitems + 32 / G - 1) / (32 / G);
+    const unsigned grid = (unsigned)std::max<long long>(
+        1, std::min<long long>((long long)device_sms() * MINB, (claims + 7) / 8));
+    k_batch_grp<WG, G, EPL, U, TV, TB, MINB><<<grid, 256, 0, st>>>(d_inst, d_items, nitems,
+                                                                   d_head);
+}
+
+// Worker shapes for the group gather (as for single products): FP32 B 32-byte
+// lane loads for 128- and 64-column tiles, 16-byte for 32; BF16 B 16-byte for
+// 128, 8-byte for 64 and 32; E4M3 B 8-byte.
+template <typename TV, typename TB>
+bool launch_batch_grp_t(int wg, const BatchInst *d_inst, const BatchItem *d_items,
+                        long long nitems, unsigned long long *d_head, cudaStream_t st)
+{
+    if constexpr (std::is_same<TB, float>::value) {
+        if (wg == 128) launch_batch_grp<128, 16, 8, 8, TV, TB, 2>(d_inst, d_items, nitems, d_head, st);
+        else if (wg == 64) launch_batch_grp<64, 8, 8, 8, TV, TB, 2>(d_inst, d_items, nitems, d_head, st);
+        else if (wg == 32) launch_batch_grp<32, 8, 4, 8, TV, TB, 3>(d_inst, d_items, nitems, d_head, st);
+        else return false;
+    } else if constexpr (sizeof(TB) == 2) {
+        if (wg == 128) launch_batch_grp<128, 16, 8, 16, TV, TB, 2>(d_inst, d_items, nitems, d_head, st);
+        else if (wg == 64) launch_batch_grp<64, 16, 4, 16, TV, TB, 3>(d_inst, d_items, nitems, d_head, st);
+        else if (wg == 32) launch_batch_grp<32, 8, 4, 16, TV, TB, 3>(d_inst, d_items, nitems, d_head, st);
+        else return false;
+    } else {
+        if (wg == 128) launch_batch_grp<128, 16, 8, 16, TV, TB, 2>(d_inst, d_items, nitems, d_head, st);
+        else if (wg == 64) launch_batch_grp<64, 8, 8, 16, TV, TB, 3>(d_inst, d_items, nitems, d_head, st);
+        else if (wg == 32) launch_batch_grp<32, 4, 8, 16, TV, TB, 3>(d_inst, d_items, nitems, d_head, st);
+        else return false;
+    }
+    return true;
+}
+
 size_t fmt_size(int f) { return f == DASPMM_F32 ? 4 : (f == DASPMM_E4M3 ? 1 : 2); }
 
 template <int WM, typename TV, typename TB>
@@ -371,9 +593,11 @@ void launch_batch_w(const BatchInst *d_inst, const BatchItem *d_items, long long
 }
 
 template <typename TV, typename TB>
-void launch_batch_t(int wmode, const BatchInst *d_inst, const BatchItem *d_items,
+void launch_batch_t(int wmode, int wgrp, const BatchInst *d_inst, const BatchItem *d_items,
                     long long nitems, unsigned long long *d_head, cudaStream_t st)
 {
+    if (DASPMM_BATCH_GRP && launch_batch_grp_t<TV, TB>(wgrp, d_inst, d_items, nitems, d_head, st))
+        return;
     if (wmode == 128) launch_batch_w<128, TV, TB>(d_inst, d_items, nitems, d_head, st);
     else if (wmode == 64) launch_batch_w<64, TV, TB>(d_inst, d_items, nitems, d_head, st);
     else if (wmode == 32) launch_batch_w<32, TV, TB>(d_inst, d_items, nitems, d_head, st);
@@ -381,6 +605,15 @@ void launch_batch_t(int wmode, const BatchInst *d_inst, const BatchItem *d_items
 }
 
 int batch_tile_width(int nv) { return nv % 128 == 0 ? 128 : (nv % 64 == 0 ? 64 : 32); }
+
+int batch_group_width(const BatchInst *h, int n)
+{
+    long long work[3] = {0, 0, 0};  // nonzeros x columns of the instances that qualify
+    for (int i = 0; i < n; ++i)
+        if (h[i].grp) work[h[i].W == 128 ? 0 : (h[i].W == 64 ? 1 : 2)] += (long long)h[i].nnz * h[i].nv;
+    const int k = work[0] >= work[1] ? (work[0] >= work[2] ? 0 : 2) : (work[1] >= work[2] ? 1 : 2);
+    return work[k] > 0 ? 128 >> k : 0;
+}
 
 bool batch_formats_ok(int vf, int bf)
 {
@@ -404,6 +637,7 @@ daspmm_status batch_fill(const daspmm_instance &s, BatchInst *d, int wcap)
     d->nr = s.nr; d->nc = s.nc; d->nnz = s.nnz; d->nv = s.nv;
     d->ldb = s.nv; d->ldc = s.nv;
     d->W = W;
+    d->grp = s.nv % W == 0 && (uintptr_t)s.B % 32 == 0 && (uintptr_t)s.C % 32 == 0;
     d->col_tiles = (s.nv + W - 1) / W;
     d->rowPtr = s.rowPtr; d->colIdx = s.colIdx; d->vals = s.values; d->B = s.B;
     d->bscale = s.b_scales; d->C = s.C; d->beta = s.beta;
@@ -468,7 +702,7 @@ daspmm_status batch_plan_async(const BatchInst *d_inst, const long long *d_begin
     return e == cudaSuccess ? DASPMM_OK : cuda_fail(e);
 }
 
-daspmm_status batch_kernel_async(int vf, int bf, int wmode, const BatchInst *d_inst,
+daspmm_status batch_kernel_async(int vf, int bf, int wmode, int wgrp, const BatchInst *d_inst,
                                  const BatchItem *d_items, long long nitems,
                                  unsigned long long *d_head, cudaStream_t st)
 {
@@ -477,15 +711,15 @@ daspmm_status batch_kernel_async(int vf, int bf, int wmode, const BatchInst *d_i
     if (e != cudaSuccess) return cuda_fail(e);
     timer_before(st);
     if (vf == DASPMM_F32 && bf == DASPMM_F32)
-        launch_batch_t<float, float>(wmode, d_inst, d_items, nitems, d_head, st);
+        launch_batch_t<float, float>(wmode, wgrp, d_inst, d_items, nitems, d_head, st);
     else if (vf == DASPMM_F32 && bf == DASPMM_BF16)
-        launch_batch_t<float, bf16>(wmode, d_inst, d_items, nitems, d_head, st);
+        launch_batch_t<float, bf16>(wmode, wgrp, d_inst, d_items, nitems, d_head, st);
     else if (vf == DASPMM_BF16 && bf == DASPMM_BF16)
-        launch_batch_t<bf16, bf16>(wmode, d_inst, d_items, nitems, d_head, st);
+        launch_batch_t<bf16, bf16>(wmode, wgrp, d_inst, d_items, nitems, d_head, st);
     else if (vf == DASPMM_F32 && bf == DASPMM_E4M3)
-        launch_batch_t<float, fp8>(wmode, d_inst, d_items, nitems, d_head, st);
+        launch_batch_t<float, fp8>(wmode, wgrp, d_inst, d_items, nitems, d_head, st);
     else
-        launch_batch_t<bf16, fp8>(wmode, d_inst, d_items, nitems, d_head, st);
+        launch_batch_t<bf16, fp8>(wmode, wgrp, d_inst, d_items, nitems, d_head, st);
     timer_after(st);
     count_launches(1);
     e = cudaGetLastError();
@@ -498,7 +732,7 @@ using namespace daspmm;
 
 struct daspmm_batch_s {
     int device = 0;
-    int ninst = 0, nv = 0, val_fmt = 0, b_fmt = 0, W = 0, chunk = 0;
+    int ninst = 0, nv = 0, val_fmt = 0, b_fmt = 0, W = 0, Wg = 0, chunk = 0;
     long long nitems = 0, total_nnz = 0;
     BatchInst *d_inst = nullptr;
     long long *d_begin = nullptr;
@@ -515,8 +749,8 @@ namespace {
 
 daspmm_status batch_launch(daspmm_batch_s *b, cudaStream_t st)
 {
-    return batch_kernel_async(b->val_fmt, b->b_fmt, b->W, b->d_inst, b->d_items, b->nitems,
-                              b->d_head, st);
+    return batch_kernel_async(b->val_fmt, b->b_fmt, b->W, b->Wg, b->d_inst, b->d_items,
+                              b->nitems, b->d_head, st);
 }
 
 void batch_free(daspmm_batch_s *b)
@@ -578,6 +812,7 @@ daspmm_status daspmm_batch_create(const daspmm_instance *inst, int n, const dasp
         b->W = (i == 0 || b->W == w) ? w : 0;  // 0: widths differ
         b->total_nnz += s.nnz;
     }
+    b->Wg = batch_group_width(hi.data(), n);
     // Tiles from each rowPtr (copied to the host once).
     std::vector<BatchTile> tiles;
     std::vector<size_t> tile_off(n), slot_off(n), cnt_off(n);

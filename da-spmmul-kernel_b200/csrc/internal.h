@@ -123,7 +123,7 @@ struct BatchInst {
     int ntiles;
     int col_tiles;  // ceil(nv / W)
     int W;
-    int pad_;
+    int grp;  // B and C 32-byte aligned and nv % W == 0: runs may take the group gather
     const int *rowPtr;
     const int *colIdx;
     const void *vals;
@@ -141,6 +141,9 @@ struct BatchItem {
 };
 
 int batch_tile_width(int nv);
+// The tile width (128, 64, 32) whose qualifying instances (BatchInst::grp)
+// hold the most nonzeros x columns, or 0: the width of the group gather.
+int batch_group_width(const BatchInst *h, int n);
 bool batch_formats_ok(int val_fmt, int b_fmt);
 // Checks one instance and fills its kernel-side row except tiles / ntiles /
 // slots / cnt (DASPMM_ERR_INVALID on a bad size, pointer or alignment).
@@ -153,10 +156,11 @@ daspmm_status batch_tune_chunks(const daspmm_instance *inst, int n, const int *c
 daspmm_status batch_plan_async(const BatchInst *d_inst, const long long *d_begin, int n,
                                BatchItem *d_items, long long nitems, cudaStream_t st);
 // Queue reset + one persistent launch.  wmode: the common tile width of all
-// instances (128, 64, 32) or 0 when they differ.
-daspmm_status batch_kernel_async(int val_fmt, int b_fmt, int wmode, const BatchInst *d_inst,
-                                 const BatchItem *d_items, long long nitems,
-                                 unsigned long long *d_head, cudaStream_t st);
+// instances (128, 64, 32) or 0 when they differ; wgrp: the tile width whose
+// runs of rows take the worker-group gather (0: none).
+daspmm_status batch_kernel_async(int val_fmt, int b_fmt, int wmode, int wgrp,
+                                 const BatchInst *d_inst, const BatchItem *d_items,
+                                 long long nitems, unsigned long long *d_head, cudaStream_t st);
 
 // Autotuner (tune.cu): the cached best configuration for a shape, or the
 // library's rule-of-thumb choice when nothing has been measured yet.

@@ -278,6 +278,7 @@ daspmm_status launch_batch(daspmm_server_s *s, Slot &sl, std::vector<Req *> &rs,
         sl.h_begin[i + 1] = sl.h_begin[i] + (long long)bi.ntiles * bi.col_tiles;
     }
     *nitems = sl.h_begin[n];
+    const int wgrp = batch_group_width(sl.h_inst, n);
     cudaError_t e = cudaMemcpyAsync(sl.d_inst, sl.h_inst, sizeof(BatchInst) * n,
                                     cudaMemcpyHostToDevice, s->stream);
     if (e == cudaSuccess)
@@ -287,8 +288,8 @@ daspmm_status launch_batch(daspmm_server_s *s, Slot &sl, std::vector<Req *> &rs,
     daspmm_status st = batch_plan_async(sl.d_inst, sl.d_begin, n, sl.d_items, *nitems,
                                         s->stream);
     if (st == DASPMM_OK)
-        st = batch_kernel_async(s->cfg.val_fmt, s->cfg.b_fmt, std::max(wmode, 0), sl.d_inst,
-                                sl.d_items, *nitems, sl.d_head, s->stream);
+        st = batch_kernel_async(s->cfg.val_fmt, s->cfg.b_fmt, std::max(wmode, 0), wgrp,
+                                sl.d_inst, sl.d_items, *nitems, sl.d_head, s->stream);
     if (st == DASPMM_OK) {
         e = cudaEventRecord(sl.ev, s->stream);
         if (e != cudaSuccess) st = cuda_fail(e);
