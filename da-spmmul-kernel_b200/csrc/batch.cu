@@ -332,7 +332,7 @@ __device__ __forceinline__ void batch_item(const BatchInst &I, const BatchTile &
 #define DASPMM_BATCH_MINB DASPMM_LEAN_MINB  // CTAs of 256 threads per SM
 #endif
 #ifndef DASPMM_BATCH_GRP
-#define DASPMM_BATCH_GRP 1  // runs of rows take the worker-group gather
+#define DASPMM_BATCH_GRP 0  // runs of rows and pieces take the worker-group gather
 #endif
 
 // WM: the tile width every instance uses, or 0 for a batch of mixed widths
