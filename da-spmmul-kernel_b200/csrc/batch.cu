@@ -332,7 +332,7 @@ __device__ __forceinline__ void batch_item(const BatchInst &I, const BatchTile &
 #define DASPMM_BATCH_MINB DASPMM_LEAN_MINB  // CTAs of 256 threads per SM
 #endif
 #ifndef DASPMM_BATCH_GRP
-#define DASPMM_BATCH_GRP 0  // runs of rows and pieces take the worker-group gather
+#define DASPMM_BATCH_GRP 1  // runs of rows and pieces take the worker-group gather
 #endif
 
 // WM: the tile width every instance uses, or 0 for a batch of mixed widths
@@ -555,9 +555,11 @@ void launch_batch_grp(const BatchInst *d_inst, const BatchItem *d_items, long lo
                                                                    d_head);
 }
 
-// Worker shapes for the group gather (as for single products): FP32 B 32-byte
-// lane loads for 128- and 64-column tiles, 16-byte for 32; BF16 B 16-byte for
-// 128, 8-byte for 64 and 32; E4M3 B 8-byte.
+// Worker shapes for the group gather: FP32 B 32-byte lane loads for 128- and
+// 64-column tiles, 16-byte for 32; BF16 B 16-byte for 128 and 64 (on the
+// 512-instance BF16 batch, N = 64: 2.48 ms against 2.94 for the 32-lane
+// kernel; 8-byte loads in 16-lane workers 3.06-3.31), 8-byte for 32; E4M3 B
+// 8-byte.
 template <typename TV, typename TB>
 bool launch_batch_grp_t(int wg, const BatchInst *d_inst, const BatchItem *d_items,
                         long long nitems, unsigned long long *d_head, cudaStream_t st)
@@ -569,7 +571,7 @@ bool launch_batch_grp_t(int wg, const BatchInst *d_inst, const BatchItem *d_item
         else return false;
     } else if constexpr (sizeof(TB) == 2) {
         if (wg == 128) launch_batch_grp<128, 16, 8, 16, TV, TB, 2>(d_inst, d_items, nitems, d_head, st);
-        else if (wg == 64) launch_batch_grp<64, 16, 4, 16, TV, TB, 3>(d_inst, d_items, nitems, d_head, st);
+        else if (wg == 64) launch_batch_grp<64, 8, 8, 16, TV, TB, 3>(d_inst, d_items, nitems, d_head, st);
         else if (wg == 32) launch_batch_grp<32, 8, 4, 16, TV, TB, 3>(d_inst, d_items, nitems, d_head, st);
         else return false;
     } else {
@@ -592,11 +594,17 @@ void launch_batch_w(const BatchInst *d_inst, const BatchItem *d_items, long long
     k_batch_spmm<WM, TV, TB><<<grid, 256, 0, st>>>(d_inst, d_items, nitems, d_head);
 }
 
+// grp: every instance shares the tile width wmode and qualifies for the
+// worker-group gather (BatchInst::grp); the group kernel then takes the batch.
+// Otherwise the 32-lane kernel: in the group kernel, items it cannot gather
+// run the 32-lane code one after another at its lower occupancy (on the
+// 64-matrix serving pool, mixed widths: capacity 56.6k against 66.5k req/s).
 template <typename TV, typename TB>
-void launch_batch_t(int wmode, int wgrp, const BatchInst *d_inst, const BatchItem *d_items,
+void launch_batch_t(int wmode, bool grp, const BatchInst *d_inst, const BatchItem *d_items,
                     long long nitems, unsigned long long *d_head, cudaStream_t st)
 {
-    if (DASPMM_BATCH_GRP && launch_batch_grp_t<TV, TB>(wgrp, d_inst, d_items, nitems, d_head, st))
+    if (DASPMM_BATCH_GRP && grp &&
+        launch_batch_grp_t<TV, TB>(wmode, d_inst, d_items, nitems, d_head, st))
         return;
     if (wmode == 128) launch_batch_w<128, TV, TB>(d_inst, d_items, nitems, d_head, st);
     else if (wmode == 64) launch_batch_w<64, TV, TB>(d_inst, d_items, nitems, d_head, st);
@@ -605,15 +613,6 @@ void launch_batch_t(int wmode, int wgrp, const BatchInst *d_inst, const BatchIte
 }
 
 int batch_tile_width(int nv) { return nv % 128 == 0 ? 128 : (nv % 64 == 0 ? 64 : 32); }
-
-int batch_group_width(const BatchInst *h, int n)
-{
-    long long work[3] = {0, 0, 0};  // nonzeros x columns of the instances that qualify
-    for (int i = 0; i < n; ++i)
-        if (h[i].grp) work[h[i].W == 128 ? 0 : (h[i].W == 64 ? 1 : 2)] += (long long)h[i].nnz * h[i].nv;
-    const int k = work[0] >= work[1] ? (work[0] >= work[2] ? 0 : 2) : (work[1] >= work[2] ? 1 : 2);
-    return work[k] > 0 ? 128 >> k : 0;
-}
 
 bool batch_formats_ok(int vf, int bf)
 {
@@ -702,7 +701,7 @@ daspmm_status batch_plan_async(const BatchInst *d_inst, const long long *d_begin
     return e == cudaSuccess ? DASPMM_OK : cuda_fail(e);
 }
 
-daspmm_status batch_kernel_async(int vf, int bf, int wmode, int wgrp, const BatchInst *d_inst,
+daspmm_status batch_kernel_async(int vf, int bf, int wmode, bool grp, const BatchInst *d_inst,
                                  const BatchItem *d_items, long long nitems,
                                  unsigned long long *d_head, cudaStream_t st)
 {
@@ -711,15 +710,15 @@ daspmm_status batch_kernel_async(int vf, int bf, int wmode, int wgrp, const Batc
     if (e != cudaSuccess) return cuda_fail(e);
     timer_before(st);
     if (vf == DASPMM_F32 && bf == DASPMM_F32)
-        launch_batch_t<float, float>(wmode, wgrp, d_inst, d_items, nitems, d_head, st);
+        launch_batch_t<float, float>(wmode, grp, d_inst, d_items, nitems, d_head, st);
     else if (vf == DASPMM_F32 && bf == DASPMM_BF16)
-        launch_batch_t<float, bf16>(wmode, wgrp, d_inst, d_items, nitems, d_head, st);
+        launch_batch_t<float, bf16>(wmode, grp, d_inst, d_items, nitems, d_head, st);
     else if (vf == DASPMM_BF16 && bf == DASPMM_BF16)
-        launch_batch_t<bf16, bf16>(wmode, wgrp, d_inst, d_items, nitems, d_head, st);
+        launch_batch_t<bf16, bf16>(wmode, grp, d_inst, d_items, nitems, d_head, st);
     else if (vf == DASPMM_F32 && bf == DASPMM_E4M3)
-        launch_batch_t<float, fp8>(wmode, wgrp, d_inst, d_items, nitems, d_head, st);
+        launch_batch_t<float, fp8>(wmode, grp, d_inst, d_items, nitems, d_head, st);
     else
-        launch_batch_t<bf16, fp8>(wmode, wgrp, d_inst, d_items, nitems, d_head, st);
+        launch_batch_t<bf16, fp8>(wmode, grp, d_inst, d_items, nitems, d_head, st);
     timer_after(st);
     count_launches(1);
     e = cudaGetLastError();
@@ -732,7 +731,8 @@ using namespace daspmm;
 
 struct daspmm_batch_s {
     int device = 0;
-    int ninst = 0, nv = 0, val_fmt = 0, b_fmt = 0, W = 0, Wg = 0, chunk = 0;
+    int ninst = 0, nv = 0, val_fmt = 0, b_fmt = 0, W = 0, chunk = 0;
+    bool grp = true;  // every instance qualifies for the worker-group gather
     long long nitems = 0, total_nnz = 0;
     BatchInst *d_inst = nullptr;
     long long *d_begin = nullptr;
@@ -749,7 +749,7 @@ namespace {
 
 daspmm_status batch_launch(daspmm_batch_s *b, cudaStream_t st)
 {
-    return batch_kernel_async(b->val_fmt, b->b_fmt, b->W, b->Wg, b->d_inst, b->d_items,
+    return batch_kernel_async(b->val_fmt, b->b_fmt, b->W, b->grp, b->d_inst, b->d_items,
                               b->nitems, b->d_head, st);
 }
 
@@ -810,9 +810,9 @@ daspmm_status daspmm_batch_create(const daspmm_instance *inst, int n, const dasp
         }
         const int w = hi[i].W;
         b->W = (i == 0 || b->W == w) ? w : 0;  // 0: widths differ
+        b->grp = b->grp && hi[i].grp;
         b->total_nnz += s.nnz;
     }
-    b->Wg = batch_group_width(hi.data(), n);
     // Tiles from each rowPtr (copied to the host once).
     std::vector<BatchTile> tiles;
     std::vector<size_t> tile_off(n), slot_off(n), cnt_off(n);

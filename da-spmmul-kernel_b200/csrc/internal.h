@@ -141,9 +141,6 @@ struct BatchItem {
 };
 
 int batch_tile_width(int nv);
-// The tile width (128, 64, 32) whose qualifying instances (BatchInst::grp)
-// hold the most nonzeros x columns, or 0: the width of the group gather.
-int batch_group_width(const BatchInst *h, int n);
 bool batch_formats_ok(int val_fmt, int b_fmt);
 // Checks one instance and fills its kernel-side row except tiles / ntiles /
 // slots / cnt (DASPMM_ERR_INVALID on a bad size, pointer or alignment).
@@ -156,9 +153,9 @@ daspmm_status batch_tune_chunks(const daspmm_instance *inst, int n, const int *c
 daspmm_status batch_plan_async(const BatchInst *d_inst, const long long *d_begin, int n,
                                BatchItem *d_items, long long nitems, cudaStream_t st);
 // Queue reset + one persistent launch.  wmode: the common tile width of all
-// instances (128, 64, 32) or 0 when they differ; wgrp: the tile width whose
-// runs of rows take the worker-group gather (0: none).
-daspmm_status batch_kernel_async(int val_fmt, int b_fmt, int wmode, int wgrp,
+// instances (128, 64, 32) or 0 when they differ; grp: with a common width,
+// every instance qualifies for the worker-group gather (BatchInst::grp).
+daspmm_status batch_kernel_async(int val_fmt, int b_fmt, int wmode, bool grp,
                                  const BatchInst *d_inst, const BatchItem *d_items,
                                  long long nitems, unsigned long long *d_head, cudaStream_t st);
 

@@ -278,7 +278,6 @@ daspmm_status launch_batch(daspmm_server_s *s, Slot &sl, std::vector<Req *> &rs,
         sl.h_begin[i + 1] = sl.h_begin[i] + (long long)bi.ntiles * bi.col_tiles;
     }
     *nitems = sl.h_begin[n];
-    const int wgrp = batch_group_width(sl.h_inst, n);
     cudaError_t e = cudaMemcpyAsync(sl.d_inst, sl.h_inst, sizeof(BatchInst) * n,
                                     cudaMemcpyHostToDevice, s->stream);
     if (e == cudaSuccess)
@@ -288,7 +287,10 @@ daspmm_status launch_batch(daspmm_server_s *s, Slot &sl, std::vector<Req *> &rs,
     daspmm_status st = batch_plan_async(sl.d_inst, sl.d_begin, n, sl.d_items, *nitems,
                                         s->stream);
     if (st == DASPMM_OK)
-        st = batch_kernel_async(s->cfg.val_fmt, s->cfg.b_fmt, std::max(wmode, 0), wgrp,
+        // the 32-lane kernel: groups are small at most arrival rates, and a
+        // group's latency is lower at its occupancy (p50 at 20k req/s 133
+        // against 202 us with the worker-group kernel)
+        st = batch_kernel_async(s->cfg.val_fmt, s->cfg.b_fmt, std::max(wmode, 0), false,
                                 sl.d_inst, sl.d_items, *nitems, sl.d_head, s->stream);
     if (st == DASPMM_OK) {
         e = cudaEventRecord(sl.ev, s->stream);

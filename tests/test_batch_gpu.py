@@ -206,3 +206,50 @@ def test_batch_tile_width_and_joint_tuner(cuda):
         assert best.chunk in (128, 512) and best.lanes_col in (32, 16) and us > 0
     with pytest.raises(D.DaspmmError):
         D.Batch(inst, lanes_col=4)
+
+
+def _offset(t):
+    """A copy of t 16 bytes past a 32-byte boundary, with the buffer that
+    holds it (keep both alive)."""
+    import torch
+    eb = t.element_size()
+    buf = torch.empty(t.numel() + 64 // eb, dtype=t.dtype, device="cuda")
+    v = buf[16 // eb: 16 // eb + t.numel()]
+    v.copy_(t)
+    assert v.data_ptr() % 32 == 16
+    return v, buf
+
+
+@pytest.mark.parametrize("vf,bf", [(D.Fmt.F32, D.Fmt.F32), (D.Fmt.F32, D.Fmt.BF16),
+                                   (D.Fmt.BF16, D.Fmt.E4M3)])
+def test_group_gather_equals_32_lane(cuda, vf, bf):
+    """Runs of whole rows and pieces of long rows take the worker-group
+    gather when B and C are 32-byte aligned and the 32-lane one when they are
+    16 bytes off: the same sums in the same order, so the batches' C are
+    bit-identical (small tiles: the hub rows are cut into many pieces)."""
+    import torch
+    rng = np.random.default_rng(19)
+    for nv in (32, 64, 128):
+        mats = _instances(rng, nv, n=12)
+        inst = _prepare(mats, nv, vf, bf, rng)
+        off, keep = [], []
+        for d in inst:
+            e = dict(d)
+            e["B"], kb = _offset(d["B"])
+            e["C"], kc = _offset(d["C"])
+            keep += [kb, kc]
+            off.append(e)
+        outs = []
+        for group in (inst, off):
+            for d in group:
+                d["C"].fill_(float("nan"))
+            b = D.Batch(group, chunk=97)
+            b.run()
+            torch.cuda.synchronize()
+            outs.append([d["C"].clone() for d in group])
+            b.close()
+        for d, x, y in zip(inst, *outs):
+            assert torch.equal(x, y), f"nv={nv} nr={d['host'].nr}: the gathers differ"
+        for d, x in zip(inst, outs[0]):
+            d["C"].copy_(x)
+            _check(d)
