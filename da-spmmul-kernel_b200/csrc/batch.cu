@@ -555,11 +555,15 @@ void launch_batch_grp(const BatchInst *d_inst, const BatchItem *d_items, long lo
                                                                    d_head);
 }
 
-// Worker shapes for the group gather: FP32 B 32-byte lane loads for 128- and
-// 64-column tiles, 16-byte for 32; BF16 B 16-byte for 128 and 64 (on the
-// 512-instance BF16 batch, N = 64: 2.48 ms against 2.94 for the 32-lane
-// kernel; 8-byte loads in 16-lane workers 3.06-3.31), 8-byte for 32; E4M3 B
-// 8-byte.
+// Worker shapes for the group gather, measured on the 512-instance batch (ms,
+// best row tile; the 32-lane kernel in brackets).  FP32 B: 32-byte lane loads
+// for 128- and 64-column tiles, 16-byte for 32 (N = 32 / 64 / 128: 1.90 /
+// 2.73 / 4.7-4.8 [2.69 / 3.15 / 4.77]).  BF16 B: 16-byte loads in 8-lane
+// workers for 64 columns, 32-byte for 128, 8-byte for 32 (FP32 values: 1.89 /
+// 2.47 / 3.78 [2.49 / 2.90 / 4.05]; BF16 values at N = 128 4.04 [3.89]).
+// E4M3 B: 8-byte loads for 64 and 32 columns (1.90 / 2.61 [2.65 / 2.94]); at
+// 128 columns every shape tried lost (4.31 [3.92]), so it keeps the 32-lane
+// kernel there.
 template <typename TV, typename TB>
 bool launch_batch_grp_t(int wg, const BatchInst *d_inst, const BatchItem *d_items,
                         long long nitems, unsigned long long *d_head, cudaStream_t st)
@@ -570,13 +574,12 @@ bool launch_batch_grp_t(int wg, const BatchInst *d_inst, const BatchItem *d_item
         else if (wg == 32) launch_batch_grp<32, 8, 4, 8, TV, TB, 3>(d_inst, d_items, nitems, d_head, st);
         else return false;
     } else if constexpr (sizeof(TB) == 2) {
-        if (wg == 128) launch_batch_grp<128, 16, 8, 16, TV, TB, 2>(d_inst, d_items, nitems, d_head, st);
+        if (wg == 128) launch_batch_grp<128, 8, 16, 8, TV, TB, 2>(d_inst, d_items, nitems, d_head, st);
         else if (wg == 64) launch_batch_grp<64, 8, 8, 16, TV, TB, 3>(d_inst, d_items, nitems, d_head, st);
         else if (wg == 32) launch_batch_grp<32, 8, 4, 16, TV, TB, 3>(d_inst, d_items, nitems, d_head, st);
         else return false;
     } else {
-        if (wg == 128) launch_batch_grp<128, 16, 8, 16, TV, TB, 2>(d_inst, d_items, nitems, d_head, st);
-        else if (wg == 64) launch_batch_grp<64, 8, 8, 16, TV, TB, 3>(d_inst, d_items, nitems, d_head, st);
+        if (wg == 64) launch_batch_grp<64, 8, 8, 16, TV, TB, 3>(d_inst, d_items, nitems, d_head, st);
         else if (wg == 32) launch_batch_grp<32, 4, 8, 16, TV, TB, 3>(d_inst, d_items, nitems, d_head, st);
         else return false;
     }
