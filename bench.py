@@ -402,8 +402,10 @@ def run_ours(args):
             nvtx.range_push("variants")
             variants = run_variants(D, A, dA, Bt, dev, peak)
             nvtx.range_pop()
-        mixed = None if args.no_mixed else run_mixed(D, A, dA, B, dev, K, peak)
-        if mixed is not None and world == 1:
+        # rank-0-only sections run at N = 1: under torchrun the other ranks wait
+        # in the closing barrier, whose process-group timeout is 120 s
+        mixed = None if (args.no_mixed or world > 1) else run_mixed(D, A, dA, B, dev, K, peak)
+        if mixed is not None:
             mixed["random_1m_deg8"] = run_mixed_random(D, dev, peak)
         batched = None if (args.no_batched or world > 1) else run_batched(D, dev)
         serving = None if (args.no_serving or world > 1) else \
