@@ -555,15 +555,15 @@ void launch_batch_grp(const BatchInst *d_inst, const BatchItem *d_items, long lo
                                                                    d_head);
 }
 
-// Worker shapes for the group gather, measured on the 512-instance batch (ms,
-// best row tile; the 32-lane kernel in brackets).  FP32 B: 32-byte lane loads
-// for 128- and 64-column tiles, 16-byte for 32 (N = 32 / 64 / 128: 1.90 /
-// 2.73 / 4.7-4.8 [2.69 / 3.15 / 4.77]).  BF16 B: 16-byte loads in 8-lane
-// workers for 64 columns, 32-byte for 128, 8-byte for 32 (FP32 values: 1.89 /
-// 2.47 / 3.78 [2.49 / 2.90 / 4.05]; BF16 values at N = 128 4.04 [3.89]).
-// E4M3 B: 8-byte loads for 64 and 32 columns (1.90 / 2.61 [2.65 / 2.94]); at
-// 128 columns every shape tried lost (4.31 [3.92]), so it keeps the 32-lane
-// kernel there.
+// Worker shapes for the group gather, measured on the 512-instance batch with
+// tiles sorted by size (ms, best row tile; the 32-lane kernel in brackets).
+// FP32 B: 32-byte lane loads for 128- and 64-column tiles, 16-byte for 32
+// (N = 32 / 64 / 128: 1.73 / 2.50 / 4.54 [2.70 / 3.19 / 4.86]).  BF16 B:
+// 16-byte loads in 8-lane workers for 64 columns, 32-byte for 128, 8-byte
+// for 32 (FP32 values: 1.64 / 2.20 / 3.39 [2.50 / 2.89 / 3.99]; BF16 values
+// 1.66 / 2.25 / 3.63 [2.50 / 2.87 / 3.88]).  E4M3 B: 8-byte loads for 64 and
+// 32 columns (1.69 / 2.31 [2.65 / 2.95]); at 128 columns every shape tried
+// lost (4.31 [3.92], tiles in row order), so it keeps the 32-lane kernel.
 template <typename TV, typename TB>
 bool launch_batch_grp_t(int wg, const BatchInst *d_inst, const BatchItem *d_items,
                         long long nitems, unsigned long long *d_head, cudaStream_t st)
@@ -691,6 +691,16 @@ void build_tiles(const int *rp, int nr, int chunk, TilePlan *out)
         for (int q = t.row0; q < r; ++q) t.npieces += rp[q + 1] == rp[q];
         out->tiles.push_back(t);
     }
+    // Longest tiles first, tiles of about the same size next to each other:
+    // the worker-group batch kernel gathers 32 / G consecutive items in step,
+    // to the longest of them (in row order 16 % of its window steps waited on
+    // a longer neighbour on the 512-instance batch), and any queue ends
+    // better with its short items last.  A tile's result does not depend on
+    // its place in the order.
+    std::stable_sort(out->tiles.begin(), out->tiles.end(),
+                     [](const BatchTile &x, const BatchTile &y) {
+                         return x.k1 - x.k0 > y.k1 - y.k0;
+                     });
 }
 
 daspmm_status batch_plan_async(const BatchInst *d_inst, const long long *d_begin, int n,
