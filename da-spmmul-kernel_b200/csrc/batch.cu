@@ -562,8 +562,9 @@ void launch_batch_grp(const BatchInst *d_inst, const BatchItem *d_items, long lo
 // 16-byte loads in 8-lane workers for 64 columns, 32-byte for 128, 8-byte
 // for 32 (FP32 values: 1.64 / 2.20 / 3.39 [2.50 / 2.89 / 3.99]; BF16 values
 // 1.66 / 2.25 / 3.63 [2.50 / 2.87 / 3.88]).  E4M3 B: 8-byte loads for 64 and
-// 32 columns (1.69 / 2.31 [2.65 / 2.95]); at 128 columns every shape tried
-// lost (4.31 [3.92], tiles in row order), so it keeps the 32-lane kernel.
+// 32 columns (1.69 / 2.31 [2.65 / 2.95]); at 128 columns the group form only
+// ties (3.93 [3.92]; 4.31 with tiles in row order), so it keeps the 32-lane
+// kernel there.
 template <typename TV, typename TB>
 bool launch_batch_grp_t(int wg, const BatchInst *d_inst, const BatchItem *d_items,
                         long long nitems, unsigned long long *d_head, cudaStream_t st)
