@@ -290,8 +290,8 @@ daspmm_status launch_batch(daspmm_server_s *s, Slot &sl, std::vector<Req *> &rs,
         // the 32-lane kernel: groups are small at most arrival rates, and a
         // group's latency is lower at its occupancy (p50 at 20k req/s 133
         // against 202 us with the worker-group kernel for uniform-width
-        // groups, 160 us when also every instance qualifies; throughput at
-        // equal p99 unchanged)
+        // groups, 160-176 us when also every instance qualifies; throughput
+        // at the tightest equal-p99 bound no higher)
         st = batch_kernel_async(s->cfg.val_fmt, s->cfg.b_fmt, std::max(wmode, 0), false,
                                 sl.d_inst, sl.d_items, *nitems, sl.d_head, s->stream);
     if (st == DASPMM_OK) {
